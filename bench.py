@@ -1,0 +1,319 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 state-vector engine on the 30-qubit random brick circuit.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|fp32] [--width k]
+    python bench.py --impl reference ...      # the reference's CPU path (parallel/AVX-512 port)
+
+Workload: 30 qubits, depth 40, every layer U3(theta, phi, lambda) on all qubits (angles
+uniform in [0, 2pi) from a SplitMix64 seed) then brick CNOTs: 1200 U3 + 580 CNOT = 1780 gates
+on a 16 GiB complex128 state.  A step is one full evolution of the resident state by the
+circuit.  value = amplitude updates per second = steps * 1780 * 2^30 / time (summed over
+ranks).  Inputs are larger than L2 (16 GiB state), so no flush is needed between steps.
+
+e2e: the same metric through the drop-in port qm_execute_host with a pinned host buffer,
+the host->device upload and device->host commit inside the timed region every step.
+
+Multi-GPU: one process per GPU, each an independent replica (the single-state path does not
+shard); timing is the max over ranks; value sums the ranks' work (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+QUBITS = 30
+DEPTH = 40
+FALLBACK_HBM_GBS = 6650.0
+
+
+def measured_peaks() -> tuple[dict, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text()), "measured"
+    return {"hbm_gbs": FALLBACK_HBM_GBS, "bf16_tflops": 1590.0}, "fallback"
+
+
+def profile_traffic(kernel_key: str) -> float | None:
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+    for f in sorted((ROOT / "profiles").glob("*.md")):
+        m = re.search(rf"traffic\[{re.escape(kernel_key)}\]:\s*([0-9.eE+]+)", f.read_text())
+        if m:
+            return float(m.group(1))
+    return None
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks and throttle reasons while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows: list[list[str]] = []
+        self._stop = threading.Event()
+        self._thread = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                for line in out.stdout.strip().splitlines():
+                    self.rows.append([x.strip() for x in line.split(",")])
+            except Exception:
+                return
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._thread.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        self._thread.join(timeout=10)
+
+    def summary(self) -> dict:
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows if len(r) >= 9 for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(sm)}
+
+
+def dist_setup(n_gpus: int):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+        return dist, rank, world, local
+    return None, 0, 1, 0
+
+
+def barrier_max(dist, value: float, local: int) -> float:
+    if dist is None:
+        return value
+    import torch
+    dev = f"cuda:{local}" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_baseline(circuit, qubits: int, sample_gates: int) -> dict:
+    """The reference's parallel/AVX-512 CPU path (oracle port) on the first gates of the workload."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import numpy as np
+
+    import oracle as orc
+    from quantummatter_b200.circuit import QuantumCircuit
+    sub = QuantumCircuit(qubits)
+    for op in circuit.Operations[:sample_gates]:
+        sub.AppendValidated(op)
+    threads = orc.hardware_threads()
+    state = np.zeros(1 << qubits, dtype=np.complex128)
+    state[0] = 1
+    orc.execute_parallel(sub, state, workers=threads)  # warm-up (first touch, pool start)
+    t0 = time.perf_counter()
+    orc.execute_parallel(sub, state, workers=threads)
+    dt = time.perf_counter() - t0
+    return {"value": sample_gates * (1 << qubits) / dt, "unit": "amp-updates/s", "cores": threads, "kind": "port",
+            "sample": f"first {sample_gates} gates (U3 layer 0) of the {qubits}-qubit circuit, AVX-512 + gate "
+                      f"blocking, {threads} worker threads, {dt:.2f} s"}
+
+
+def run_reference(args) -> None:
+    """`--impl reference`: the reference's own CPU implementation (parallel/AVX-512 port) on this
+    arm's workload; each step is a bounded sample of the circuit."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from quantummatter_b200.workloads import brick_circuit
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import numpy as np
+
+    import oracle as orc
+    from quantummatter_b200.circuit import QuantumCircuit
+    circuit = brick_circuit(QUBITS, DEPTH)
+    sample = 4
+    sub = QuantumCircuit(QUBITS)
+    for op in circuit.Operations[:sample]:
+        sub.AppendValidated(op)
+    threads = orc.hardware_threads()
+    state = np.zeros(1 << QUBITS, dtype=np.complex128)
+    state[0] = 1
+    for _ in range(args.warmup):
+        orc.execute_parallel(sub, state, workers=threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        orc.execute_parallel(sub, state, workers=threads)
+    dt = time.perf_counter() - t0
+    value = args.steps * sample * (1 << QUBITS) / dt
+    line = {
+        "impl": "reference", "metric": "amp-updates/s at 30q", "value": value, "unit": "amp-updates/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "brick circuit, 30 qubits, depth 40, U3 + CNOT, 1780 gates, complex128 state",
+                   "qubits": QUBITS, "depth": DEPTH, "gates": len(circuit.Operations),
+                   "sample_per_step": f"first {sample} gates of the circuit on the full 2^30 state"},
+        "cpu_baseline": {"value": value, "unit": "amp-updates/s", "cores": threads, "kind": "port",
+                         "sample": f"first {sample} gates per step, {threads} threads, AVX-512 + gate blocking"},
+        "e2e": {"value": value, "unit": "amp-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="native", choices=["native", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--width", type=int, default=0, help="fusion width (block qubits); 1 = one launch per gate")
+    ap.add_argument("--qubits", type=int, default=QUBITS)
+    ap.add_argument("--depth", type=int, default=DEPTH)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    dist, rank, world, local = dist_setup(args.gpus)
+    import numpy as np
+
+    from quantummatter_b200.backend import (FP32, FP64, B200BackendOptions, B200Context, B200StateVectorBackend,
+                                            DeviceState, Plan)
+    from quantummatter_b200.workloads import brick_circuit
+
+    qubits, depth = args.qubits, args.depth
+    precision = FP32 if args.precision == "fp32" else FP64
+    elem = 8 if precision == FP32 else 16
+    circuit = brick_circuit(qubits, depth)
+    gates = len(circuit.Operations)
+    amps = 1 << qubits
+    ctx = B200Context(B200BackendOptions(DeviceIndex=local, DeviceMemoryBudgetBytes=80 << 30,
+                                         StagingMemoryBudgetBytes=80 << 30, EnableProfiling=True,
+                                         FusionWidth=args.width))
+    plan = Plan(ctx, circuit, precision, args.width)
+    passes, launches, planned_bytes = plan.stats()
+    state = DeviceState(ctx, qubits, precision)
+
+    for _ in range(args.warmup):
+        plan.execute(state)
+    barrier_max(dist, 0.0, local)
+    device_seconds = []
+    with ClockSampler(local) as clocks:
+        t_wall = time.perf_counter()
+        for _ in range(args.steps):
+            prof = plan.execute(state, profile=True)
+            device_seconds.append(prof.DeviceEvolutionSeconds)
+        wall = time.perf_counter() - t_wall
+    total = sum(device_seconds)
+    total_max = barrier_max(dist, total, local)
+    ms_per_step = 1e3 * total_max / args.steps
+    value = world * args.steps * gates * amps / total_max
+
+    peaks, peak_kind = measured_peaks()
+    hbm_peak = float(peaks.get("hbm_gbs", FALLBACK_HBM_GBS))
+    per_launch_s = total / (args.steps * launches)
+    bytes_per_launch = planned_bytes / launches
+    achieved_gbs = bytes_per_launch / per_launch_s / 1e9
+    kernel_key = f"k_fused_{args.precision}_k{plan_width(passes, qubits, precision, args.width)}_{qubits}q" if passes else \
+        f"k_gate_{args.precision}_{qubits}q"
+    traffic = profile_traffic(kernel_key)
+
+    # FP64/FP32 arithmetic actually issued: 16 real FMA-flops per amplitude per dense 2x2 gate
+    dense = sum(1 for op in circuit.Operations if int(op.Kind) not in (1, 9, 10, 11, 16))
+    flops = dense * amps * 8 * 2
+    e2e = None
+    if not args.no_e2e and precision == FP64:
+        backend = B200StateVectorBackend(context=ctx)
+        host = ctx.host_array(amps)
+        host.array[:] = 0
+        host.array[0] = 1
+        e2e_steps = max(2, args.steps // 2)
+        backend.Execute(circuit, host.array)  # warm-up of the port (allocation of its device buffer)
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            backend.Execute(circuit, host.array)
+        dt = barrier_max(dist, time.perf_counter() - t0, local)
+        e2e = {"value": world * e2e_steps * gates * amps / dt, "unit": "amp-updates/s",
+               "h2d_bytes_per_step": elem * amps, "d2h_bytes_per_step": elem * amps,
+               "ms_per_step": 1e3 * dt / e2e_steps, "path": "qm_execute_host (drop-in port), pinned host buffer"}
+        host.free()
+        backend.Dispose()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        state.Dispose()
+        cpu = cpu_baseline(circuit, qubits, 8)
+
+    if rank == 0:
+        line = {
+            "metric": "amp-updates/s at 30q", "value": value, "unit": "amp-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if precision == FP32 else "f64",
+            "data": "synthetic",
+            "config": {"workload": f"brick circuit, {qubits} qubits, depth {depth}, U3 + CNOT, {gates} gates, "
+                                   f"{'complex64' if precision == FP32 else 'complex128'} state resident in HBM",
+                       "qubits": qubits, "depth": depth, "gates": gates, "precision": args.precision,
+                       "fusion": f"{passes} fused passes (block width {plan_width(passes, qubits, precision, args.width)})"
+                       if passes else f"{launches} per-gate launches",
+                       "l2": f"inputs larger than L2 ({elem * amps / 2**30:.0f} GiB state); no flush",
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "achieved": achieved_gbs, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": achieved_gbs / hbm_peak, "traffic": traffic, "peak_source": peak_kind,
+                         "kernel": kernel_key, "algorithmic_bytes_per_launch": bytes_per_launch,
+                         "launch_ms": 1e3 * per_launch_s,
+                         "fp_alu_tflops": flops * args.steps / total / 1e12},
+            "gpu_launches": args.steps * launches,
+            "clocks": clocks.summary(),
+            "wall_s_timed": wall,
+        }
+        if e2e:
+            line["e2e"] = e2e
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    plan.Dispose()
+    try:
+        state.Dispose()
+    except Exception:
+        pass
+    ctx.Dispose()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def plan_width(passes: int, qubits: int, precision: int, width: int) -> int:
+    if width:
+        return width
+    return min(13 if precision == 1 else 12, qubits)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,285 @@
+/*
+ * qm_b200.h -- C ABI of libqmb200.so, the B200 (sm_100a) state-vector engine behind
+ * QuantumMatter's execution-backend ports.
+ *
+ * Everything here is plain C: fixed-width integers, doubles, opaque handles and
+ * caller-owned arrays.  Amplitude arrays on the host are interleaved complex128
+ * (re, im), the layout of System.Numerics.Complex[].  Every call returns a qm_status;
+ * qm_last_error() gives the message of the last failure on the calling thread.
+ *
+ * Reference interfaces replaced (paths inside the olgerd007/QuantumMatter project):
+ *   IStateVectorBackend.Execute        src/QuantumMatter.Core/IStateVectorBackend.cs:13
+ *   INoiseChannelBackend.Apply         src/QuantumMatter.Core/Noise/INoiseChannelBackend.cs:13-14
+ *   CudaStateVectorBackend             src/QuantumMatter.Infrastructure/CudaStateVectorBackend.cs:21-216
+ *   PreparedStateVectorGate.Prepare    src/QuantumMatter.Infrastructure/PreparedStateVectorGate.cs:13-70
+ * and, as additive device-resident APIs, the host-side loops of
+ *   StateVector.ExpectationValue/ExpectationEnergy  src/QuantumMatter.Core/StateVector.Observations.cs:107-141,
+ *                                                   src/QuantumMatter.Core/StateVector.Energy.cs:10-46
+ *   StateVector.MeasureAll                          src/QuantumMatter.Core/StateVector.cs:106-153
+ *   StateVectorSimulator.Run sampling               src/QuantumMatter.Application/StateVectorSimulator.cs:44-90
+ */
+#ifndef QM_B200_H
+#define QM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QM_ABI_VERSION 1
+
+/* Status codes.  The right-hand comment is the exception the reference raises for
+ * the same condition, which is what a .NET shim maps the code to. */
+typedef enum qm_status {
+    QM_OK = 0,
+    QM_E_ARG = 1,          /* ArgumentException / ArgumentNullException */
+    QM_E_BUDGET = 2,       /* InvalidOperationException: state exceeds a memory budget (CudaStateVectorBackend.cs:120-124) */
+    QM_E_OOM = 3,          /* OutOfMemoryException: device or pinned allocation failed */
+    QM_E_DEVICE = 4,       /* PlatformNotSupportedException / CUDA runtime error (CudaStateVectorBackend.cs:31-35) */
+    QM_E_CANCELLED = 5,    /* OperationCanceledException */
+    QM_E_TIMEOUT = 6,      /* a bounded device wait ran out */
+    QM_E_MASS = 7,         /* InvalidOperationException: no finite positive probability mass */
+    QM_E_DISPOSED = 8,     /* ObjectDisposedException */
+    QM_E_UNSUPPORTED = 9,  /* NotSupportedException: unknown gate kind */
+    QM_E_RANGE = 10        /* ArgumentOutOfRangeException */
+} qm_status;
+
+/* Element type of a device state. */
+typedef enum qm_precision {
+    QM_FP64 = 0,           /* complex128, the drop-in form */
+    QM_FP32 = 1            /* complex64; reductions, masses and CDFs stay FP64 */
+} qm_precision;
+
+/* ---------------------------------------------------------------- gates */
+
+/* GateKind numbering (src/QuantumMatter.Core/QuantumCircuit.cs:4-40). */
+enum {
+    QM_GATE_H = 0, QM_GATE_X = 1, QM_GATE_Y = 2, QM_GATE_Z = 3, QM_GATE_S = 4, QM_GATE_T = 5,
+    QM_GATE_RX = 6, QM_GATE_RY = 7, QM_GATE_RZ = 8, QM_GATE_CNOT = 9, QM_GATE_SWAP = 10,
+    QM_GATE_I = 11, QM_GATE_SDG = 12, QM_GATE_TDG = 13, QM_GATE_PHASE = 14,
+    QM_GATE_UNITARY = 15, QM_GATE_TOFFOLI = 16
+};
+
+/* One GateOperation record (QuantumCircuit.cs:49-51).  unitary holds the row-major
+ * m00, m01, m10, m11 entries as (re, im) pairs and is read only for QM_GATE_UNITARY. */
+typedef struct qm_operation {
+    int32_t kind;
+    int32_t target;
+    int32_t control;         /* -1 when absent; the first SWAP operand for QM_GATE_SWAP */
+    int32_t second_control;  /* -1 when absent */
+    double angle;
+    double unitary[8];
+} qm_operation;              /* 88 bytes */
+
+/* StateVectorKernelKind (PreparedStateVectorGate.cs:6). */
+enum {
+    QM_KERNEL_IDENTITY = 0, QM_KERNEL_MATRIX = 1, QM_KERNEL_HADAMARD = 2,
+    QM_KERNEL_EXCHANGE = 3, QM_KERNEL_DIAGONAL = 4, QM_KERNEL_SWAP = 5
+};
+
+/* One prepared gate, the record PreparedStateVectorGate holds (PreparedStateVectorGate.cs:9-11):
+ * coefficients are evaluated once on the host.  Matrix/Hadamard: [a b; c d] on the
+ * target pair.  Diagonal: a on target-zero, d on target-one.  Exchange: X.  Swap:
+ * exchanges the target and swap_control qubits.  A gate acts only where every bit of
+ * control_mask is set. */
+typedef struct qm_gate {
+    int32_t kernel;
+    int32_t target;
+    uint32_t control_mask;
+    int32_t swap_control;    /* -1 unless kernel == QM_KERNEL_SWAP */
+    double a[2], b[2], c[2], d[2];
+} qm_gate;                   /* 80 bytes */
+
+/* ---------------------------------------------------------------- options */
+
+/* CudaBackendOptions (src/QuantumMatter.Infrastructure/CudaBackendOptions.cs:4-21) plus the
+ * engine's own knobs.  Zero-initialise, then set fields; qm_options_default fills the
+ * reference defaults (512 MiB budgets, device 0). */
+typedef struct qm_options {
+    int32_t device_index;
+    int32_t enable_profiling;       /* fills qm_profile in the *_profiled calls */
+    int64_t device_budget_bytes;    /* maximum bytes of device states held by the context */
+    int64_t staging_budget_bytes;   /* maximum pinned host staging bytes */
+    int32_t fusion_width;           /* 0 = planner default; 1 = one launch per gate; else block qubits */
+    int32_t reserved[7];
+} qm_options;
+
+/* CudaExecutionProfile (CudaBackendOptions.cs:35): device time of the gate sequence
+ * (CUDA events, launch gaps included, transfers excluded), state bytes, launches. */
+typedef struct qm_profile {
+    double device_seconds;
+    double transfer_seconds;        /* host<->device copies of the host-buffer entry points */
+    int64_t state_bytes;
+    int32_t kernel_launches;
+    int32_t passes;                 /* fused passes (0 on the per-gate path) */
+    int64_t planned_bytes;          /* DRAM bytes the plan reads+writes */
+} qm_profile;
+
+typedef struct qm_device_info {
+    int32_t index;
+    int32_t sm_count;
+    int32_t major, minor;
+    int32_t driver_version;
+    int32_t reserved;
+    int64_t memory_bytes;
+    char name[256];
+} qm_device_info;
+
+typedef struct qm_context qm_context;
+typedef struct qm_state qm_state;
+typedef struct qm_plan qm_plan;
+
+/* ---------------------------------------------------------------- runtime */
+
+int32_t qm_abi_version(void);
+/* Copies the calling thread's last error message (NUL-terminated, truncated). */
+int32_t qm_last_error(char* buffer, size_t size);
+void qm_options_default(qm_options* options);
+/* CudaStateVectorBackend.GetDevices (CudaStateVectorBackend.cs:70-85). */
+int32_t qm_device_count(int32_t* count);
+int32_t qm_device_info_get(int32_t index, qm_device_info* info);
+
+/* CudaStateVectorBackend constructor / Dispose (CudaStateVectorBackend.cs:21-64,191-216).
+ * QM_E_DEVICE when no device exists, QM_E_RANGE for a bad device index. */
+int32_t qm_context_create(const qm_options* options, qm_context** context);
+int32_t qm_context_destroy(qm_context* context);
+
+/* Pinned host memory from the context's device, for callers that keep amplitude
+ * arrays in page-locked memory (the copies then run at full PCIe/C2C rate). */
+int32_t qm_host_alloc(qm_context* context, int64_t bytes, void** pointer);
+int32_t qm_host_free(qm_context* context, void* pointer);
+
+/* PreparedStateVectorGate.Prepare for `count` operations on a `qubits`-qubit register,
+ * after the builder validation of QuantumCircuit.cs:97-134. */
+int32_t qm_prepare_gates(const qm_operation* operations, int32_t count, int32_t qubits, qm_gate* gates);
+
+/* ---------------------------------------------------------------- drop-in port */
+
+/* IStateVectorBackend.Execute on a host buffer (CudaStateVectorBackend.ExecuteCore,
+ * CudaStateVectorBackend.cs:103-188): validates length == 2^qubits (QM_E_ARG), checks
+ * the budgets before touching the buffer (QM_E_BUDGET), uploads, runs every gate in
+ * insertion order on the device, downloads and commits.  *cancel (may be NULL) is
+ * polled before work, between launch chunks of at most 32 gates and before the
+ * commit; QM_E_CANCELLED or any failure before the commit leaves the buffer unchanged.
+ * profile may be NULL. */
+int32_t qm_execute_host(qm_context* context, int32_t qubits, const qm_operation* operations,
+                        int32_t count, double* amplitudes, int64_t length,
+                        const volatile int32_t* cancel, qm_profile* profile);
+
+/* INoiseChannelBackend.Apply on a host buffer (CpuNoiseChannelBackend.cs:10-145).
+ * kind: 0 bit flip, 1 phase flip, 2 depolarizing, 3 amplitude damping
+ * (src/QuantumMatter.Core/Noise/NoiseChannel.cs:4-14).  Random draws come from the
+ * caller's generator through next_double (System.Random.NextDouble in the .NET shim),
+ * consumed exactly where the reference consumes them: none when p == 0, none for a
+ * flip with p == 1, none for damping when either branch has zero mass. */
+typedef double (*qm_next_double_fn)(void* user);
+int32_t qm_noise_apply_host(qm_context* context, int32_t kind, double probability, int32_t target,
+                            double* amplitudes, int64_t length, qm_next_double_fn next_double,
+                            void* user, const volatile int32_t* cancel);
+
+/* ---------------------------------------------------------------- device states */
+
+/* Allocates a device state of 2^qubits amplitudes (qubits in [1,30]) set to |0...0>.
+ * QM_E_BUDGET when the context's device budget would be exceeded. */
+int32_t qm_state_create(qm_context* context, int32_t qubits, int32_t precision, qm_state** state);
+int32_t qm_state_destroy(qm_state* state);
+int32_t qm_state_reset(qm_state* state);                       /* StateVector.Reset */
+int32_t qm_state_upload(qm_state* state, const double* amplitudes, int64_t length);
+int32_t qm_state_download(qm_state* state, double* amplitudes, int64_t length);
+/* Device address of the amplitude array (complex128 or complex64, interleaved). */
+int32_t qm_state_device_pointer(qm_state* state, void** pointer);
+
+/* Runs prepared gates in order on a device state.  fusion_width as in qm_options
+ * (0 = context default).  profile may be NULL. */
+int32_t qm_execute(qm_state* state, const qm_gate* gates, int32_t count, int32_t fusion_width,
+                   qm_profile* profile);
+
+/* A reusable fused schedule for one gate list: planned once, executed many times. */
+int32_t qm_plan_create(qm_context* context, int32_t qubits, int32_t precision, const qm_gate* gates,
+                       int32_t count, int32_t fusion_width, qm_plan** plan);
+int32_t qm_plan_execute(qm_plan* plan, qm_state* state, qm_profile* profile);
+/* passes, kernel launches and planned DRAM bytes of one execution. */
+int32_t qm_plan_stats(const qm_plan* plan, int32_t* passes, int32_t* launches, int64_t* planned_bytes);
+int32_t qm_plan_destroy(qm_plan* plan);
+
+/* Host-only inspection of the fused schedule the planner builds for a gate list (no
+ * device needed): pass headers and the op program each pass's kernel interprets.
+ * Counts are always written; records are written when the arrays are large enough.
+ * The records mirror the engine's internal layout (op codes: 0 stage change, 1 complex
+ * matrix, 2 real matrix, 3 X, 4 diagonal, 5 negate, 6 swap). */
+typedef struct qm_fused_pass_info {
+    int32_t block_qubits;
+    int32_t op_begin, op_count;
+    int32_t qubits[14];      /* ascending; local bit i of a block index is qubits[i] */
+    uint32_t block_mask;
+    int32_t stages;
+} qm_fused_pass_info;        /* 76 bytes */
+
+typedef struct qm_fused_op_info {
+    int32_t code;
+    int32_t reg, reg2;       /* register bits of the current stage layout */
+    int32_t local;           /* local bit of a diagonal target, -1 outside the block */
+    uint32_t cmask_local;    /* controls (and negate target) as local-index bits */
+    uint32_t cmask_outer;    /* controls (and negate target) outside the block, global bits */
+    uint32_t target_outer;   /* outside-the-block diagonal target, global bit */
+    int32_t flags;           /* bit0: a == 1, bit1: d == 1 */
+    int32_t reg_pos[4];      /* stage change: local bit of each register bit */
+    double coef[8];          /* a, b, c, d as (re, im) */
+} qm_fused_op_info;          /* 112 bytes */
+
+int32_t qm_plan_program(int32_t qubits, int32_t precision, const qm_gate* gates, int32_t count,
+                        int32_t fusion_width, int32_t* passes, qm_fused_pass_info* pass_records,
+                        int32_t max_passes, int32_t* ops, qm_fused_op_info* op_records, int32_t max_ops,
+                        int64_t* planned_bytes);
+
+/* ---------------------------------------------------------------- noise primitives */
+
+/* FP64 compensated masses of target-zero and target-one amplitudes
+ * (CpuNoiseChannelBackend.cs:88-106). */
+int32_t qm_qubit_masses(qm_state* state, int32_t target, double* zero_mass, double* one_mass);
+/* Pauli branch on the target: 1 = X, 2 = Y, 3 = Z (CpuNoiseChannelBackend.cs:59-80). */
+int32_t qm_apply_pauli(qm_state* state, int32_t target, int32_t pauli);
+/* Damping branch (CpuNoiseChannelBackend.cs:118-142): jump != 0 writes
+ * psi0 = jump_scale * psi1, psi1 = 0; otherwise psi0 *= scale, psi1 *= stay_scale. */
+int32_t qm_apply_damping(qm_state* state, int32_t target, int32_t jump, double scale,
+                         double jump_scale, double stay_scale);
+
+/* ---------------------------------------------------------------- observables */
+
+/* One Pauli term: PauliString masks (src/QuantumMatter.Core/PauliString.cs:37-39) and the
+ * real coefficient of a PauliTerm (src/QuantumMatter.Core/Observables/PauliTerm.cs:7-13). */
+typedef struct qm_pauli_term {
+    uint32_t flip_mask;      /* X or Y positions */
+    uint32_t sign_mask;      /* Z or Y positions */
+    int32_t y_count;
+    int32_t reserved;
+    double coefficient;
+} qm_pauli_term;             /* 24 bytes */
+
+/* One fused pass: per_term[t] = <psi|P_t|psi> / <psi|psi> for every term (coefficients
+ * ignored), *mass = <psi|psi>, FP64 accumulation.  QM_E_MASS when the mass is not
+ * finite and positive or a term sum is not finite. */
+int32_t qm_expectation_pauli(qm_state* state, const qm_pauli_term* terms, int32_t count,
+                             double* per_term, double* mass);
+/* StateVector.ExpectationEnergy: sum of c_t <P_t> over nonzero coefficients in term order
+ * with Neumaier compensation.  An empty term list still validates the mass. */
+int32_t qm_expectation_energy(qm_state* state, const qm_pauli_term* terms, int32_t count,
+                              double* energy);
+
+/* ---------------------------------------------------------------- sampling */
+
+/* StateVector.MeasureAll: u is the caller's NextDouble draw; collapses the state to the
+ * sampled basis state with amplitude +1.  *ambiguous is set when u*total lies within the
+ * device/host rounding margin of a CDF boundary (the outcome is then still the device's). */
+int32_t qm_measure_all(qm_state* state, double u, int64_t* outcome, int32_t* ambiguous);
+/* StateVectorSimulator.Run terminal sampling: FP64 CDF, draw*total, strict upper-bound
+ * search per shot, without collapse.  *ambiguous counts shots near a boundary. */
+int32_t qm_sample(qm_state* state, const double* draws, int32_t shots, int64_t* outcomes,
+                  int32_t* ambiguous);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* QM_B200_H */

@@ -1,0 +1,164 @@
+// qm_internal.h -- declarations shared by the host runtime and the CUDA kernels of
+// libqmb200.so.  Not part of the public ABI (that is include/qm_b200.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "qm_b200.h"
+
+namespace qm {
+
+// ---------------------------------------------------------------- errors
+void set_error(const std::string& message);
+int32_t fail(int32_t status, const std::string& message);
+int32_t cuda_fail(cudaError_t err, const char* what);
+
+#define QM_CUDA(call)                                         \
+    do {                                                      \
+        cudaError_t qm_err_ = (call);                         \
+        if (qm_err_ != cudaSuccess) return ::qm::cuda_fail(qm_err_, #call); \
+    } while (0)
+
+// ---------------------------------------------------------------- device gate record
+// Device form of a prepared gate: masks instead of qubit numbers (DeviceGate,
+// CudaStateVectorKernel.cs:24-34), coefficients as doubles.
+struct DevGate {
+    int32_t kernel;
+    uint32_t target_bit;
+    uint32_t control_mask;
+    uint32_t swap_bit;
+    int32_t target;
+    int32_t swap_control;
+    int32_t a_is_one;   // diagonal zero-phase is exactly 1: the target-zero half is untouched
+    int32_t d_is_one;
+    double a[2], b[2], c[2], d[2];
+};
+DevGate to_dev_gate(const qm_gate& g);
+
+// ---------------------------------------------------------------- fused-pass program
+// One fused pass touches a block of 2^k amplitudes per CTA: the local index bits are
+// the pass's block qubits q[0..k) (ascending, always including the lowest qubits so
+// that global reads come in contiguous runs), the other qubits are fixed per CTA.
+// Each thread keeps 2^R amplitudes in registers; a stage selects which R local bits
+// are register bits, and every gate of the stage either targets a register bit or is
+// diagonal.  Stage changes go through shared memory.
+constexpr int kRegBits = 4;
+constexpr int kMaxBlockQubits = 14;
+
+enum OpCode : int32_t {
+    OP_STAGE = 0,      // new register layout: reg_pos[0..R) local bit positions
+    OP_MATRIX = 1,     // complex 2x2 on register bit `reg`
+    OP_MATRIX_REAL = 2,// real 2x2 (imaginary parts all zero)
+    OP_EXCHANGE = 3,   // X on register bit `reg`
+    OP_DIAG = 4,       // diagonal: a on bit-zero, d on bit-one of local bit `local` (or outer bit)
+    OP_NEGATE = 5,     // amplitude *= -1 where all of (local_mask | target) set: CZ, Z
+    OP_SWAP = 6,       // exchange register bits `reg` and `reg2`
+};
+
+struct FusedOp {
+    int32_t code;
+    int32_t reg;            // register bit (0..R) of the target, or -1
+    int32_t reg2;           // second register bit for OP_SWAP
+    int32_t local;          // local bit of a diagonal target, -1 when the target is outside the block
+    uint32_t cmask_local;   // controls inside the block, as local-index bits
+    uint32_t cmask_outer;   // controls outside the block, as global-index bits
+    uint32_t target_outer;  // outer target bit of a diagonal (global), 0 when local
+    int32_t flags;          // bit0: a == 1, bit1: d == 1 (diagonal)
+    int32_t reg_pos[kRegBits];  // OP_STAGE: local bit positions of the register bits
+    double coef[8];         // a, b, c, d as (re, im)
+};
+
+struct FusedPass {
+    int32_t k;                      // block qubits
+    int32_t op_begin, op_count;     // range in the plan's op array
+    int32_t q[kMaxBlockQubits];     // block qubits, ascending
+    uint32_t block_mask;            // OR of 1<<q[i]
+    int32_t stages;                 // number of register layouts (>= 1)
+};
+
+struct Plan {
+    int32_t qubits = 0;
+    int32_t precision = QM_FP64;
+    int32_t width = 0;              // 1: per-gate path
+    std::vector<DevGate> gates;     // per-gate path
+    std::vector<FusedPass> passes;  // fused path
+    std::vector<FusedOp> ops;
+    FusedOp* d_ops = nullptr;       // device copy of ops
+    int64_t planned_bytes = 0;
+    int32_t launches = 0;
+};
+
+// Builds the fused schedule (qm_planner.cpp).  Returns false with a message on error.
+bool plan_fused(const std::vector<qm_gate>& gates, int qubits, int precision, int width, Plan& plan,
+                std::string& error);
+int default_block_qubits(int qubits, int precision);
+
+// ---------------------------------------------------------------- launchers (qm_kernels.cu)
+cudaError_t launch_gate(void* amps, int qubits, int precision, const DevGate& g, cudaStream_t s);
+cudaError_t launch_fused(void* amps, int qubits, int precision, const FusedPass& p, const FusedOp* d_ops,
+                         cudaStream_t s);
+cudaError_t launch_reset(void* amps, int qubits, int precision, cudaStream_t s);
+cudaError_t launch_convert_from_f64(void* dst_f32, const double* src_f64, int64_t n, cudaStream_t s);
+cudaError_t launch_convert_to_f64(double* dst_f64, const void* src_f32, int64_t n, cudaStream_t s);
+// FP64 partial sums: writes `blocks` partial (sum, compensation) pairs into scratch.
+cudaError_t launch_masses(const void* amps, int qubits, int precision, int target, double* scratch,
+                          int* blocks_out, cudaStream_t s);
+cudaError_t launch_pauli(void* amps, int qubits, int precision, int target, int pauli, cudaStream_t s);
+cudaError_t launch_damping(void* amps, int qubits, int precision, int target, int jump, double scale,
+                           double jump_scale, double stay_scale, cudaStream_t s);
+// Expectation: per-block partial sums [blocks][terms + 1] (last column = mass).
+struct DevPauli { uint32_t flip, sign; int32_t phase; int32_t pad; };
+cudaError_t launch_expectation(const void* amps, int qubits, int precision, const DevPauli* d_terms,
+                               int terms, double* scratch, int* blocks_out, cudaStream_t s);
+cudaError_t launch_finish_sums(const double* partials, int blocks, int columns, double* out,
+                               cudaStream_t s);
+// Sampling: per-block probability sums, then searches.
+cudaError_t launch_block_probs(const void* amps, int qubits, int precision, double* block_sums,
+                               int64_t* block_last, int* blocks_out, int* chunk_out, cudaStream_t s);
+cudaError_t launch_search(const void* amps, int qubits, int precision, const double* block_prefix,
+                          int blocks, int chunk, const double* targets, int shots, double margin,
+                          int64_t* out, cudaStream_t s);
+cudaError_t launch_collapse(void* amps, int qubits, int precision, int64_t outcome, cudaStream_t s);
+
+}  // namespace qm
+
+// ---------------------------------------------------------------- handles
+struct qm_context {
+    int32_t device = 0;
+    int32_t sm_count = 0;
+    int32_t profiling = 0;
+    int32_t fusion_width = 0;
+    int64_t device_budget = 0;
+    int64_t staging_budget = 0;
+    int64_t device_in_use = 0;
+    bool disposed = false;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+    std::recursive_mutex mu;
+    // growable scratch (reduction partials, small uploads)
+    void* scratch = nullptr;
+    size_t scratch_bytes = 0;
+    double* host_scratch = nullptr;   // pinned, for small downloads
+    size_t host_scratch_bytes = 0;
+    // pinned staging for pageable host buffers (qm_execute_host)
+    void* staging = nullptr;
+    size_t staging_bytes = 0;
+};
+
+struct qm_state {
+    qm_context* ctx = nullptr;
+    int32_t qubits = 0;
+    int32_t precision = QM_FP64;
+    void* amps = nullptr;
+    int64_t bytes = 0;
+};
+
+struct qm_plan {
+    qm_context* ctx = nullptr;
+    qm::Plan plan;
+};

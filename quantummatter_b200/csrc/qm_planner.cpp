@@ -1,0 +1,301 @@
+// qm_planner.cpp -- gate-fusion planner of libqmb200.so.
+//
+// Turns an ordered list of prepared gates into fused passes for qm_fused.cu.  The
+// reference executes one launch per non-identity gate (CudaStateVectorBackend.cs:145-160)
+// and, on the CPU, reuses tiles only across adjacent same-target uncontrolled gates
+// (ParallelCpuStateVectorBackend.cs:109-181).  Here a pass may hold any gates whose
+// non-diagonal targets fit in the pass's block of k qubits, in any order the gates'
+// commutation allows:
+//   * a gate acts non-diagonally ("x role") on its target (and both SWAP operands) and
+//     diagonally ("z role") on its controls; a diagonal gate is z role on every qubit;
+//   * two gates commute when every qubit they share is z role in both (both are then
+//     block-diagonal in the shared qubits' computational basis);
+//   * a gate may move ahead of a skipped gate only if they commute.
+// Diagonal gates never need block or register space: their phase is a function of the
+// global index, which every amplitude knows.
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "qm_internal.h"
+
+namespace qm {
+
+namespace {
+
+struct GInfo {
+    qm_gate g;
+    bool diag;
+    uint32_t touch;  // every qubit the gate reads
+    uint32_t xmask;  // qubits acted on non-diagonally
+    uint32_t zmask;  // qubits acted on diagonally
+    uint32_t need;   // qubits that must be register bits
+};
+
+inline int popc(uint32_t x) { return __builtin_popcount(x); }
+
+GInfo classify(const qm_gate& g) {
+    GInfo gi{};
+    gi.g = g;
+    uint32_t tb = 1u << g.target;
+    uint32_t sb = g.kernel == QM_KERNEL_SWAP ? (1u << g.swap_control) : 0u;
+    gi.touch = tb | sb | g.control_mask;
+    if (g.kernel == QM_KERNEL_DIAGONAL) {
+        gi.diag = true;
+        gi.xmask = 0;
+        gi.zmask = gi.touch;
+        gi.need = 0;
+    } else {
+        gi.diag = false;
+        gi.xmask = tb | sb;
+        gi.zmask = g.control_mask;
+        gi.need = tb | sb;
+    }
+    return gi;
+}
+
+inline bool blocked(const GInfo& g, uint32_t bx, uint32_t bz) { return (g.touch & bx) || (g.xmask & bz); }
+
+inline bool is_exact(const double* v, double re, double im) { return v[0] == re && v[1] == im; }
+
+}  // namespace
+
+DevGate to_dev_gate(const qm_gate& g) {
+    DevGate d{};
+    d.kernel = g.kernel;
+    d.target = g.target;
+    d.target_bit = 1u << g.target;
+    d.control_mask = g.control_mask;
+    d.swap_control = g.swap_control;
+    d.swap_bit = g.kernel == QM_KERNEL_SWAP ? (1u << g.swap_control) : 0u;
+    d.a_is_one = is_exact(g.a, 1.0, 0.0);
+    d.d_is_one = is_exact(g.d, 1.0, 0.0);
+    std::memcpy(d.a, g.a, sizeof d.a);
+    std::memcpy(d.b, g.b, sizeof d.b);
+    std::memcpy(d.c, g.c, sizeof d.c);
+    std::memcpy(d.d, g.d, sizeof d.d);
+    return d;
+}
+
+int default_block_qubits(int qubits, int precision) {
+    int k = precision == QM_FP32 ? 13 : 12;
+    return std::min(k, qubits);
+}
+
+bool plan_fused(const std::vector<qm_gate>& gates, int qubits, int precision, int width, Plan& plan,
+                std::string& error) {
+    plan.qubits = qubits;
+    plan.precision = precision;
+    plan.passes.clear();
+    plan.ops.clear();
+    plan.gates.clear();
+    plan.planned_bytes = 0;
+    plan.launches = 0;
+    const int64_t elem = precision == QM_FP32 ? 8 : 16;
+    const int64_t n = int64_t(1) << qubits;
+
+    const int kmax = precision == QM_FP32 ? 13 : 12;
+    int k = width <= 0 ? default_block_qubits(qubits, precision) : std::min(width, kmax);
+    k = std::min(k, qubits);
+    // Per-gate path: requested explicitly (width 1) or the state is too small for a block
+    // of at least 9 qubits (32 threads of 16 registers).
+    if (width == 1 || k < 9) {
+        plan.width = 1;
+        for (const qm_gate& g : gates) {
+            if (g.kernel == QM_KERNEL_IDENTITY) continue;
+            DevGate d = to_dev_gate(g);
+            if (d.kernel == QM_KERNEL_DIAGONAL && d.a_is_one && d.d_is_one) continue;
+            plan.gates.push_back(d);
+            int active = popc(d.target_bit | d.control_mask | d.swap_bit);
+            int64_t pairs = n >> active;
+            int64_t touched = 2 * pairs;
+            if (d.kernel == QM_KERNEL_DIAGONAL && (d.a_is_one || d.d_is_one)) touched = pairs;
+            plan.planned_bytes += 2 * touched * elem;
+        }
+        plan.launches = (int32_t)plan.gates.size();
+        return true;
+    }
+    plan.width = k;
+
+    std::vector<GInfo> remaining;
+    remaining.reserve(gates.size());
+    for (const qm_gate& g : gates) {
+        if (g.kernel == QM_KERNEL_IDENTITY) continue;
+        if (g.kernel == QM_KERNEL_DIAGONAL && is_exact(g.a, 1.0, 0.0) && is_exact(g.d, 1.0, 0.0)) continue;
+        if (g.kernel == QM_KERNEL_SWAP && (g.swap_control < 0 || g.swap_control == g.target)) {
+            error = "swap operands must be distinct";
+            return false;
+        }
+        remaining.push_back(classify(g));
+    }
+
+    // Low qubits always in the block: 8 complex128 or 16 complex64 = one 128-byte run.
+    const int low_bits = precision == QM_FP32 ? 4 : 3;
+    const uint32_t low_mask = (1u << low_bits) - 1u;
+
+    while (!remaining.empty()) {
+        uint32_t Q = low_mask;
+        uint32_t bx = 0, bz = 0;
+        std::vector<GInfo> absorbed, rest;
+        for (const GInfo& g : remaining) {
+            if (!blocked(g, bx, bz)) {
+                uint32_t nq = Q | g.need;
+                if (popc(nq) <= k) {
+                    Q = nq;
+                    absorbed.push_back(g);
+                    continue;
+                }
+            }
+            rest.push_back(g);
+            bx |= g.xmask;
+            bz |= g.zmask;
+        }
+        if (absorbed.empty()) {
+            error = "planner made no progress";
+            return false;
+        }
+        // fill the block to k qubits with the lowest unused qubits
+        for (int q = 0; q < qubits && popc(Q) < k; ++q) Q |= 1u << q;
+
+        FusedPass pass{};
+        pass.k = k;
+        pass.block_mask = Q;
+        int local_of[32];
+        for (int i = 0; i < 32; ++i) local_of[i] = -1;
+        int nb = 0;
+        for (int q = 0; q < qubits; ++q)
+            if (Q & (1u << q)) {
+                local_of[q] = nb;
+                pass.q[nb++] = q;
+            }
+        pass.op_begin = (int32_t)plan.ops.size();
+
+        // stage planning inside the pass (capacity R register bits)
+        const uint32_t canonical = ((1u << kRegBits) - 1u) << (k - kRegBits);  // local bits
+        uint32_t layout = canonical;                                       // current local register bits
+        std::vector<GInfo> pending = absorbed;
+        int stages = 0;
+        while (!pending.empty()) {
+            uint32_t P = 0;  // global qubits needed in registers
+            uint32_t sbx = 0, sbz = 0;
+            std::vector<GInfo> stage_gates, later;
+            for (const GInfo& g : pending) {
+                if (!blocked(g, sbx, sbz)) {
+                    if (g.diag) {
+                        stage_gates.push_back(g);
+                        continue;
+                    }
+                    uint32_t np = P | g.need;
+                    if (popc(np) <= kRegBits) {
+                        P = np;
+                        stage_gates.push_back(g);
+                        continue;
+                    }
+                }
+                later.push_back(g);
+                sbx |= g.xmask;
+                sbz |= g.zmask;
+            }
+            // local register mask: needed qubits, then the current layout's bits (no data
+            // movement when it already fits), then the highest local bits
+            uint32_t Pl = 0;
+            for (int q = 0; q < qubits; ++q)
+                if (P & (1u << q)) Pl |= 1u << local_of[q];
+            uint32_t new_layout;
+            if ((Pl & ~layout) == 0) {
+                new_layout = layout;
+            } else {
+                new_layout = Pl;
+                for (int b = k - 1; b >= 0 && popc(new_layout) < kRegBits; --b)
+                    if ((layout & (1u << b)) && !(new_layout & (1u << b))) new_layout |= 1u << b;
+                for (int b = k - 1; b >= 0 && popc(new_layout) < kRegBits; --b) new_layout |= 1u << b;
+            }
+            if (new_layout != layout) {
+                FusedOp st{};
+                st.code = OP_STAGE;
+                int m = 0;
+                for (int b = 0; b < k; ++b)
+                    if (new_layout & (1u << b)) st.reg_pos[m++] = b;
+                plan.ops.push_back(st);
+                layout = new_layout;
+                ++stages;
+            }
+            int reg_of_local[32];
+            for (int i = 0; i < 32; ++i) reg_of_local[i] = -1;
+            {
+                int m = 0;
+                for (int b = 0; b < k; ++b)
+                    if (layout & (1u << b)) reg_of_local[b] = m++;
+            }
+            for (const GInfo& gi : stage_gates) {
+                const qm_gate& g = gi.g;
+                FusedOp op{};
+                op.reg = op.reg2 = -1;
+                op.local = -1;
+                for (int q = 0; q < qubits; ++q) {
+                    if (!(g.control_mask & (1u << q))) continue;
+                    if (local_of[q] >= 0) op.cmask_local |= 1u << local_of[q];
+                    else op.cmask_outer |= 1u << q;
+                }
+                std::memcpy(&op.coef[0], g.a, 16);
+                std::memcpy(&op.coef[2], g.b, 16);
+                std::memcpy(&op.coef[4], g.c, 16);
+                std::memcpy(&op.coef[6], g.d, 16);
+                if (gi.diag) {
+                    bool a1 = is_exact(g.a, 1.0, 0.0), d1 = is_exact(g.d, 1.0, 0.0);
+                    int lt = local_of[g.target];
+                    if (a1 && is_exact(g.d, -1.0, 0.0)) {
+                        op.code = OP_NEGATE;
+                        if (lt >= 0) op.cmask_local |= 1u << lt;
+                        else op.cmask_outer |= 1u << g.target;
+                    } else {
+                        op.code = OP_DIAG;
+                        op.local = lt;
+                        op.target_outer = lt >= 0 ? 0u : (1u << g.target);
+                        op.flags = (a1 ? 1 : 0) | (d1 ? 2 : 0);
+                    }
+                } else if (g.kernel == QM_KERNEL_EXCHANGE) {
+                    op.code = OP_EXCHANGE;
+                    op.reg = reg_of_local[local_of[g.target]];
+                } else if (g.kernel == QM_KERNEL_SWAP) {
+                    op.code = OP_SWAP;
+                    op.reg = reg_of_local[local_of[g.target]];
+                    op.reg2 = reg_of_local[local_of[g.swap_control]];
+                } else {
+                    bool real = g.a[1] == 0 && g.b[1] == 0 && g.c[1] == 0 && g.d[1] == 0;
+                    op.code = real ? OP_MATRIX_REAL : OP_MATRIX;
+                    op.reg = reg_of_local[local_of[g.target]];
+                }
+                if ((op.code == OP_MATRIX || op.code == OP_MATRIX_REAL || op.code == OP_EXCHANGE) && op.reg < 0) {
+                    error = "planner placed a gate outside the register layout";
+                    return false;
+                }
+                if (op.code == OP_SWAP && (op.reg < 0 || op.reg2 < 0)) {
+                    error = "planner placed a swap outside the register layout";
+                    return false;
+                }
+                plan.ops.push_back(op);
+            }
+            pending.swap(later);
+        }
+        if (layout != canonical) {
+            FusedOp st{};
+            st.code = OP_STAGE;
+            int m = 0;
+            for (int b = 0; b < k; ++b)
+                if (canonical & (1u << b)) st.reg_pos[m++] = b;
+            plan.ops.push_back(st);
+            ++stages;
+        }
+        pass.op_count = (int32_t)plan.ops.size() - pass.op_begin;
+        pass.stages = stages;
+        plan.passes.push_back(pass);
+        plan.planned_bytes += 2 * n * elem;
+        remaining.swap(rest);
+    }
+    plan.launches = (int32_t)plan.passes.size();
+    return true;
+}
+
+}  // namespace qm

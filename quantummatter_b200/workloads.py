@@ -1,0 +1,63 @@
+"""Seeded synthetic workloads of the benchmark configurations.
+
+All inputs are synthetic (the reference measures on synthetic circuits only,
+benchmarks/QuantumMatter.Benchmarks/CudaBenchmarks.cs:118-146).  Angles come from a
+SplitMix64 stream so every run, test and benchmark sees identical circuits.
+"""
+from __future__ import annotations
+
+import math
+
+from .circuit import QuantumCircuit, u3
+
+MASK64 = (1 << 64) - 1
+DEFAULT_SEED = 20260101
+
+
+class SplitMix64:
+    """SplitMix64 (Steele, Lea, Flood 2014) with doubles from the top 53 bits."""
+
+    def __init__(self, seed: int):
+        self.state = seed & MASK64
+
+    def next_u64(self) -> int:
+        self.state = (self.state + 0x9E3779B97F4A7C15) & MASK64
+        z = self.state
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & MASK64
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & MASK64
+        return z ^ (z >> 31)
+
+    def next_double(self) -> float:
+        return (self.next_u64() >> 11) * (1.0 / (1 << 53))
+
+    def uniform(self, lo: float, hi: float) -> float:
+        return lo + (hi - lo) * self.next_double()
+
+    def normal(self, mu: float = 0.0, sigma: float = 1.0) -> float:
+        u1 = 1.0 - self.next_double()
+        u2 = self.next_double()
+        return mu + sigma * math.sqrt(-2.0 * math.log(u1)) * math.cos(2 * math.pi * u2)
+
+
+def brick_circuit(qubits: int, depth: int, seed: int = DEFAULT_SEED) -> QuantumCircuit:
+    """Random U3 + brick-pattern CNOT circuit.
+
+    Each layer: U3(theta, phi, lambda) on every qubit with angles uniform in [0, 2pi), then
+    CNOT(2i, 2i+1) on even layers and CNOT(2i+1, 2i+2) on odd layers.  20 qubits x 20 layers
+    gives 400 U3 + 190 CNOT = 590 gates; 30 x 40 gives 1200 + 580 = 1780.
+    """
+    rng = SplitMix64(seed)
+    c = QuantumCircuit(qubits)
+    two_pi = 2 * math.pi
+    for layer in range(depth):
+        for q in range(qubits):
+            theta, phi, lam = rng.uniform(0, two_pi), rng.uniform(0, two_pi), rng.uniform(0, two_pi)
+            c.U(q, u3(theta, phi, lam))
+        start = 0 if layer % 2 == 0 else 1
+        for q in range(start, qubits - 1, 2):
+            c.CNot(q, q + 1)
+    return c
+
+
+def gate_count(circuit: QuantumCircuit) -> int:
+    return len(circuit.Operations)

@@ -1,0 +1,96 @@
+"""Executes a fused schedule from qm_plan_program on the CPU with numpy (test infrastructure).
+
+The emulator follows the semantics the fused kernel implements: per pass, every CTA owns
+the amplitudes whose block-qubit bits vary and whose other bits are fixed; ops act on the
+block in order; a stage change only moves data between threads, so it merely changes which
+local bit each register index names.  Comparing the emulated result with the oracle checks
+the planner (gate placement, reordering, register and mask translation) without a GPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from quantummatter_b200 import _lib
+
+OP_STAGE, OP_MATRIX, OP_MATRIX_REAL, OP_EXCHANGE, OP_DIAG, OP_NEGATE, OP_SWAP = range(7)
+
+
+def program(qubits: int, precision: int, gates, count: int, width: int):
+    lib = _lib.load()
+    np_, no, nbytes = C.c_int32(), C.c_int32(), C.c_int64()
+    _lib.check(lib.qm_plan_program(qubits, precision, gates, count, width, C.byref(np_), None, 0, C.byref(no), None, 0,
+                                   C.byref(nbytes)))
+    passes = (_lib.FusedPassInfo * max(1, np_.value))()
+    ops = (_lib.FusedOpInfo * max(1, no.value))()
+    _lib.check(lib.qm_plan_program(qubits, precision, gates, count, width, C.byref(np_), passes, np_.value,
+                                   C.byref(no), ops, no.value, C.byref(nbytes)))
+    return list(passes)[:np_.value], list(ops)[:no.value], nbytes.value
+
+
+def deposit(values: np.ndarray, mask: int) -> np.ndarray:
+    out = np.zeros_like(values)
+    bit = 0
+    for b in range(32):
+        if mask >> b & 1:
+            out |= ((values >> bit) & 1) << b
+            bit += 1
+    return out
+
+
+def emulate(state: np.ndarray, qubits: int, passes, ops, reg_bits: int = 4) -> np.ndarray:
+    s = state.copy()
+    full = (1 << qubits) - 1
+    for p in passes:
+        k = p.block_qubits
+        outer_mask = full & ~p.block_mask
+        ctas = np.arange(1 << (qubits - k), dtype=np.int64)
+        outer = deposit(ctas, outer_mask)
+        local = np.arange(1 << k, dtype=np.int64)
+        idx = outer[:, None] | deposit(local, p.block_mask)[None, :]
+        blk = s[idx]
+        canonical = list(range(k - reg_bits, k))
+        layout = canonical
+        for op in ops[p.op_begin:p.op_begin + p.op_count]:
+            if op.code == OP_STAGE:
+                layout = list(op.reg_pos)
+                assert len(set(layout)) == reg_bits and all(0 <= b < k for b in layout)
+                continue
+            cta_ok = (outer & op.cmask_outer) == op.cmask_outer
+            ctl = (local & op.cmask_local) == op.cmask_local
+            a, b, c, d = (complex(op.coef[2 * i], op.coef[2 * i + 1]) for i in range(4))
+            if op.code in (OP_MATRIX, OP_MATRIX_REAL, OP_EXCHANGE):
+                lb = layout[op.reg]
+                j0 = local[((local >> lb) & 1 == 0) & ctl]
+                j1 = j0 | (1 << lb)
+                x, y = blk[:, j0].copy(), blk[:, j1].copy()
+                if op.code == OP_EXCHANGE:
+                    nx, ny = y, x
+                else:
+                    nx, ny = a * x + b * y, c * x + d * y
+                blk[np.ix_(cta_ok, j0)] = nx[cta_ok]
+                blk[np.ix_(cta_ok, j1)] = ny[cta_ok]
+            elif op.code == OP_SWAP:
+                l1, l2 = layout[op.reg], layout[op.reg2]
+                j0 = local[((local >> l1) & 1 == 1) & ((local >> l2) & 1 == 0) & ctl]
+                j1 = j0 ^ (1 << l1) ^ (1 << l2)
+                x, y = blk[:, j0].copy(), blk[:, j1].copy()
+                blk[np.ix_(cta_ok, j0)] = y[cta_ok]
+                blk[np.ix_(cta_ok, j1)] = x[cta_ok]
+            elif op.code == OP_NEGATE:
+                sel = local[ctl]
+                blk[np.ix_(cta_ok, sel)] *= -1
+            elif op.code == OP_DIAG:
+                if op.local >= 0:
+                    bit = np.broadcast_to(((local >> op.local) & 1).astype(bool)[None, :], blk.shape)
+                else:
+                    bit = np.broadcast_to(((outer & op.target_outer) != 0)[:, None], blk.shape)
+                mask = cta_ok[:, None] & ctl[None, :]
+                phase = np.where(bit, d, a)
+                blk = np.where(mask, blk * phase, blk)
+            else:
+                raise AssertionError(f"unknown op {op.code}")
+        assert layout == canonical, "a pass must end in the canonical layout"
+        s[idx] = blk
+    return s

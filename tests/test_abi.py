@@ -1,0 +1,139 @@
+"""The C-ABI library on the CPU: it loads, exports every declared entry point, keeps the
+struct layouts of include/qm_b200.h, prepares gates exactly as the oracle does, and its
+fusion planner produces programs that the CPU emulator runs to the oracle's result."""
+from __future__ import annotations
+
+import ctypes as C
+import re
+
+import numpy as np
+import pytest
+
+import oracle as orc
+import plan_emulator as pe
+from circuits import random_circuit, random_state
+from conftest import ROOT
+from quantummatter_b200 import _lib
+from quantummatter_b200.circuit import QuantumCircuit, prepare
+from quantummatter_b200.errors import ArgumentError, ArgumentOutOfRangeError, NotSupportedError
+from quantummatter_b200.workloads import brick_circuit
+
+HEADER = ROOT / "include" / "qm_b200.h"
+
+
+def declared_symbols() -> set[str]:
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return set(re.findall(r"\b(qm_[a-z0-9_]+)\s*\(", text))
+
+
+def test_library_exports_every_declared_entry_point():
+    lib = _lib.load()
+    names = declared_symbols()
+    assert len(names) >= 30
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+    assert names == set(_lib.SIGNATURES), "the ctypes binding covers exactly the header"
+    assert lib.qm_abi_version() == 1
+
+
+def test_struct_layouts_match_the_header():
+    assert C.sizeof(_lib.Operation) == 88
+    assert C.sizeof(_lib.Gate) == 80
+    assert C.sizeof(_lib.PauliTermC) == 24
+    assert C.sizeof(_lib.FusedOpInfo) == 112
+    assert C.sizeof(_lib.FusedPassInfo) == 76
+    assert C.sizeof(_lib.Options) == 56
+
+
+def test_prepared_gates_equal_the_oracle_bit_for_bit():
+    """qm_prepare_gates restates PreparedStateVectorGate.Prepare with the host libm."""
+    for seed in range(8):
+        c = random_circuit(6, 200, seed=seed)
+        got, n = prepare(c)
+        want = orc.prepare(c)
+        assert C.string_at(C.addressof(got), n * 80) == C.string_at(C.addressof(want), n * 80)
+
+
+def test_prepare_validates_like_the_circuit_builders():
+    lib = _lib.load()
+    ops = (_lib.Operation * 1)()
+    gates = (_lib.Gate * 1)()
+    ops[0].kind, ops[0].target, ops[0].control, ops[0].second_control = 9, 1, 1, -1
+    with pytest.raises(ArgumentError):
+        _lib.check(lib.qm_prepare_gates(ops, 1, 2, gates))
+    ops[0].control = 5
+    with pytest.raises(ArgumentOutOfRangeError):
+        _lib.check(lib.qm_prepare_gates(ops, 1, 2, gates))
+    ops[0].kind, ops[0].control = 42, -1
+    with pytest.raises(NotSupportedError):
+        _lib.check(lib.qm_prepare_gates(ops, 1, 2, gates))
+    ops[0].kind, ops[0].angle = 6, float("nan")
+    with pytest.raises(ArgumentOutOfRangeError):
+        _lib.check(lib.qm_prepare_gates(ops, 1, 2, gates))
+
+
+def _emulate_against_oracle(circuit: QuantumCircuit, width: int, precision: int = 0, seed: int = 0) -> int:
+    n = circuit.QubitCount
+    gates, count = prepare(circuit)
+    passes, ops, planned = pe.program(n, precision, gates, count, width)
+    psi = random_state(n, seed)
+    got = pe.emulate(psi, n, passes, ops)
+    want = orc.execute(circuit, psi)
+    assert np.max(np.abs(got - want)) <= 1e-12
+    return len(passes)
+
+
+@pytest.mark.parametrize("width", [9, 10])
+def test_planner_programs_reproduce_the_oracle_on_random_circuits(width):
+    for seed in range(4):
+        c = random_circuit(12, 160, seed=200 + seed)
+        _emulate_against_oracle(c, width, seed=seed)
+
+
+def test_planner_handles_controls_and_diagonals_outside_the_block():
+    c = QuantumCircuit(12)
+    for q in range(12):
+        c.H(q)
+    c.CZ(11, 0).CPhase(10, 11, 0.3).Toffoli(11, 10, 2).CRy(11, 1, 0.7).Rz(11, 1.1).Swap(0, 5)
+    c.Controlled(c.Operations[0].Kind, 9, 3).Phase(10, -0.4).CNot(0, 11).Z(11).S(10).T(9)
+    for q in range(12):
+        c.Rx(q, 0.1 * q)
+    _emulate_against_oracle(c, 9, seed=3)
+
+
+def test_planner_brick_circuit_pass_counts_and_bytes():
+    c = brick_circuit(16, 8, seed=11)
+    gates, count = prepare(c)
+    passes, ops, planned = pe.program(16, 0, gates, count, 12)
+    assert planned == len(passes) * 2 * (16 << 16)
+    assert len(passes) < count / 8, "fusion must cut launches by an order of magnitude"
+    psi = random_state(16, 5)
+    got = pe.emulate(psi, 16, passes, ops)
+    assert np.max(np.abs(got - orc.execute(c, psi))) <= 1e-12
+
+
+def test_per_gate_width_counts_one_launch_per_gate():
+    c = brick_circuit(10, 3, seed=1)
+    gates, count = prepare(c)
+    np_, no, nbytes = C.c_int32(), C.c_int32(), C.c_int64()
+    _lib.check(_lib.load().qm_plan_program(10, 0, gates, count, 1, C.byref(np_), None, 0, C.byref(no), None, 0,
+                                           C.byref(nbytes)))
+    assert np_.value == 0 and no.value == 0
+    # 30 dense U3 (2S each) + 5 + 4 + 5 CNOT (S each), S = 16 * 2^10
+    assert nbytes.value == 30 * 2 * (16 << 10) + 14 * (16 << 10)
+
+
+def test_no_device_behaviour_on_a_cpu_host():
+    """Without a GPU, device discovery returns an empty list and context creation reports
+    PlatformNotSupported (CudaStateVectorBackend.cs:31-35)."""
+    lib = _lib.load()
+    n = C.c_int32(-1)
+    assert lib.qm_device_count(C.byref(n)) == 0
+    if n.value > 0:
+        pytest.skip("a CUDA device is visible")
+    o = _lib.Options()
+    lib.qm_options_default(C.byref(o))
+    h = C.c_void_p()
+    assert lib.qm_context_create(C.byref(o), C.byref(h)) == 4
+    assert "No compatible NVIDIA CUDA device" in _lib.last_error()
