@@ -214,20 +214,23 @@ typedef struct qm_fused_pass_info {
     int32_t op_begin, op_count;
     int32_t qubits[14];      /* ascending; local bit i of a block index is qubits[i] */
     uint32_t block_mask;
-    int32_t stages;
-} qm_fused_pass_info;        /* 76 bytes */
+    int32_t stages;          /* register layouts used by the pass */
+    int8_t reg_in[4];        /* local register bits of the load layout */
+    int8_t reg_out[4];       /* local register bits of the store layout */
+} qm_fused_pass_info;        /* 84 bytes */
 
 typedef struct qm_fused_op_info {
-    int32_t code;
-    int32_t reg, reg2;       /* register bits of the current stage layout */
-    int32_t local;           /* local bit of a diagonal target, -1 outside the block */
-    uint32_t cmask_local;    /* controls (and negate target) as local-index bits */
+    uint8_t code;
+    int8_t reg, reg2;        /* register bits of the current stage layout */
+    int8_t local;            /* local bit of a diagonal target, -1 outside the block */
+    int8_t reg_pos[4];       /* stage change: local bit of each register bit */
+    uint16_t cmask_local;    /* controls (and negate target) as local-index bits */
+    uint16_t flags;          /* bit0: a == 1, bit1: d == 1 */
     uint32_t cmask_outer;    /* controls (and negate target) outside the block, global bits */
     uint32_t target_outer;   /* outside-the-block diagonal target, global bit */
-    int32_t flags;           /* bit0: a == 1, bit1: d == 1 */
-    int32_t reg_pos[4];      /* stage change: local bit of each register bit */
+    uint32_t reserved;
     double coef[8];          /* a, b, c, d as (re, im) */
-} qm_fused_op_info;          /* 112 bytes */
+} qm_fused_op_info;          /* 88 bytes */
 
 int32_t qm_plan_program(int32_t qubits, int32_t precision, const qm_gate* gates, int32_t count,
                         int32_t fusion_width, int32_t* passes, qm_fused_pass_info* pass_records,

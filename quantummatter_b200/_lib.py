@@ -6,12 +6,15 @@ is no CPU fallback anywhere in this package.
 from __future__ import annotations
 
 import ctypes as C
+import os
 import threading
 from pathlib import Path
 
 from .errors import raise_for_status
 
-LIB_PATH = Path(__file__).resolve().parent / "libqmb200.so"
+# QM_B200_LIBRARY selects another build of the same ABI (e.g. one compiled with other
+# register-blocking parameters); by default the in-tree library is used.
+LIB_PATH = Path(os.environ.get("QM_B200_LIBRARY") or Path(__file__).resolve().parent / "libqmb200.so")
 
 # ---------------------------------------------------------------- structs (layouts of qm_b200.h)
 
@@ -52,13 +55,15 @@ class PauliTermC(C.Structure):
 
 class FusedPassInfo(C.Structure):
     _fields_ = [("block_qubits", C.c_int32), ("op_begin", C.c_int32), ("op_count", C.c_int32),
-                ("qubits", C.c_int32 * 14), ("block_mask", C.c_uint32), ("stages", C.c_int32)]
+                ("qubits", C.c_int32 * 14), ("block_mask", C.c_uint32), ("stages", C.c_int32),
+                ("reg_in", C.c_int8 * 4), ("reg_out", C.c_int8 * 4)]
 
 
 class FusedOpInfo(C.Structure):
-    _fields_ = [("code", C.c_int32), ("reg", C.c_int32), ("reg2", C.c_int32), ("local", C.c_int32),
-                ("cmask_local", C.c_uint32), ("cmask_outer", C.c_uint32), ("target_outer", C.c_uint32),
-                ("flags", C.c_int32), ("reg_pos", C.c_int32 * 4), ("coef", C.c_double * 8)]
+    _fields_ = [("code", C.c_uint8), ("reg", C.c_int8), ("reg2", C.c_int8), ("local", C.c_int8),
+                ("reg_pos", C.c_int8 * 4), ("cmask_local", C.c_uint16), ("flags", C.c_uint16),
+                ("cmask_outer", C.c_uint32), ("target_outer", C.c_uint32), ("reserved", C.c_uint32),
+                ("coef", C.c_double * 8)]
 
 
 NEXT_DOUBLE_FN = C.CFUNCTYPE(C.c_double, C.c_void_p)

@@ -225,18 +225,11 @@ int32_t build_plan(qm_context* ctx, int32_t qubits, int32_t precision, const qm_
     std::string err;
     if (width == 0) width = ctx->fusion_width;
     if (!plan_fused(list, qubits, precision, width, plan, err)) return fail(QM_E_ARG, "planner: " + err);
-    if (!plan.ops.empty()) {
-        QM_CUDA(cudaMalloc(&plan.d_ops, plan.ops.size() * sizeof(FusedOp)));
-        QM_CUDA(cudaMemcpyAsync(plan.d_ops, plan.ops.data(), plan.ops.size() * sizeof(FusedOp),
-                                cudaMemcpyHostToDevice, ctx->stream));
-    }
     return QM_OK;
 }
 
-void free_plan(Plan& plan) {
-    if (plan.d_ops) cudaFree(plan.d_ops);
-    plan.d_ops = nullptr;
-}
+// Plans hold host memory only (each pass's program travels as a kernel parameter).
+void free_plan(Plan& plan) { plan.ops.clear(); }
 
 // Launches the plan on `amps`.  With a cancel flag the stream is synchronised every 32
 // launches and the flag polled, as the reference bounds queued work
@@ -258,7 +251,7 @@ int32_t run_plan(qm_context* ctx, const Plan& plan, void* amps, const volatile i
         }
     } else {
         for (const FusedPass& p : plan.passes) {
-            QM_CUDA(launch_fused(amps, plan.qubits, plan.precision, p, plan.d_ops, ctx->stream));
+            QM_CUDA(launch_fused(amps, plan.qubits, plan.precision, p, plan.ops.data(), ctx->stream));
             int32_t rc = chunk_boundary();
             if (rc) return rc;
         }

@@ -10,6 +10,11 @@
 // qubit, applied by index test).  Controls may sit on any qubit: inside the block they
 // are a per-amplitude predicate, outside it they are uniform per CTA.  Between stages
 // the block is exchanged through shared memory with an XOR swizzle on the 128-byte rows.
+// The load and store use the first and last stage layouts directly whenever those keep
+// the lowest qubits on thread bits (coalesced), so most passes have no extra exchange.
+//
+// The op program is a __grid_constant__ kernel parameter: every op field is a uniform
+// load from the constant bank, so interpreting the program costs no memory traffic.
 //
 // The arithmetic per gate is the pair update of CudaStateVectorKernel.cs:63-75
 // (a*x + b*y, c*x + d*y) in the state's precision with fused multiply-adds.
@@ -25,10 +30,17 @@ namespace {
 constexpr int R = kRegBits;
 constexpr int NR = 1 << R;
 
+template <int MAXOPS>
 struct FusedLaunch {
-    uint32_t outer_mask;  // qubits outside the block
-    int32_t op_begin, op_count;
-    int32_t q[kMaxBlockQubits];
+    uint32_t outer_mask;        // qubits outside the block
+    uint32_t thread_in;         // global mask of the block qubits that are thread bits at load
+    uint32_t thread_out;        // ... at store
+    int32_t op_count;
+    uint32_t reg_in_g[R];       // global bit of each register bit at load
+    uint32_t reg_out_g[R];      // ... at store
+    int32_t reg_in_l[R];        // local positions of the load layout
+    int32_t pad[R];
+    FusedOp ops[MAXOPS];
 };
 
 // Shared-memory slot of local index j: the low row bits are XORed with a fold of the
@@ -57,18 +69,19 @@ struct Layout {
     }
 };
 
-template <typename T, int M>
-__device__ __forceinline__ void op_matrix(Cx<T> (&a)[NR], const FusedOp& op, const Layout& L, bool real) {
-    const T ar = (T)op.coef[0], ai = (T)op.coef[1], br = (T)op.coef[2], bi = (T)op.coef[3];
-    const T cr = (T)op.coef[4], ci = (T)op.coef[5], dr = (T)op.coef[6], di = (T)op.coef[7];
+template <typename T, int M, bool REAL, bool CTRL>
+__device__ __forceinline__ void op_matrix(Cx<T> (&a)[NR], const FusedOp& op, const Layout& L) {
+    const T ar = (T)op.coef[0], br = (T)op.coef[2], cr = (T)op.coef[4], dr = (T)op.coef[6];
+    const T ai = REAL ? (T)0 : (T)op.coef[1], bi = REAL ? (T)0 : (T)op.coef[3];
+    const T ci = REAL ? (T)0 : (T)op.coef[5], di = REAL ? (T)0 : (T)op.coef[7];
     const uint32_t cm = op.cmask_local;
 #pragma unroll
     for (int i = 0; i < NR; ++i) {
         if ((i >> M) & 1) continue;
         const int k = i | (1 << M);
-        if (cm != 0 && (L.local(i) & cm) != cm) continue;
+        if (CTRL && (L.local(i) & cm) != cm) continue;
         Cx<T> x = a[i], y = a[k];
-        if (real) {
+        if (REAL) {
             a[i] = Cx<T>{ar * x.re + br * y.re, ar * x.im + br * y.im};
             a[k] = Cx<T>{cr * x.re + dr * y.re, cr * x.im + dr * y.im};
         } else {
@@ -78,6 +91,22 @@ __device__ __forceinline__ void op_matrix(Cx<T> (&a)[NR], const FusedOp& op, con
     }
 }
 
+template <typename T, bool REAL, bool CTRL>
+__device__ __forceinline__ void op_matrix_any(Cx<T> (&a)[NR], const FusedOp& op, const Layout& L) {
+    switch (op.reg) {
+    case 0: op_matrix<T, 0, REAL, CTRL>(a, op, L); break;
+    case 1: op_matrix<T, 1, REAL, CTRL>(a, op, L); break;
+#if QM_REG_BITS > 3
+    case 2: op_matrix<T, 2, REAL, CTRL>(a, op, L); break;
+    default: op_matrix<T, 3, REAL, CTRL>(a, op, L); break;
+#else
+    default: op_matrix<T, 2, REAL, CTRL>(a, op, L); break;
+#endif
+    }
+}
+
+// X on register bit M where the control lies outside the registers (or there is none):
+// a per-amplitude predicate.
 template <typename T, int M>
 __device__ __forceinline__ void op_exchange(Cx<T> (&a)[NR], const FusedOp& op, const Layout& L) {
     const uint32_t cm = op.cmask_local;
@@ -85,11 +114,56 @@ __device__ __forceinline__ void op_exchange(Cx<T> (&a)[NR], const FusedOp& op, c
     for (int i = 0; i < NR; ++i) {
         if ((i >> M) & 1) continue;
         const int k = i | (1 << M);
-        if (cm != 0 && (L.local(i) & cm) != cm) continue;
-        Cx<T> x = a[i];
-        a[i] = a[k];
-        a[k] = x;
+        const bool on = (L.local(i) & cm) == cm;
+        Cx<T> x = a[i], y = a[k];
+        a[i] = on ? y : x;
+        a[k] = on ? x : y;
     }
+}
+
+// X on register bit M controlled by register bit MC: the swapped pairs are known at compile
+// time, so the op is a fixed register permutation (plus a predicate for any other control).
+template <typename T, int M, int MC>
+__device__ __forceinline__ void op_exchange_rc(Cx<T> (&a)[NR], const FusedOp& op, const Layout& L) {
+    const uint32_t cm = op.cmask_local & ~L.pm[MC];
+#pragma unroll
+    for (int i = 0; i < NR; ++i) {
+        if (((i >> M) & 1) || !((i >> MC) & 1)) continue;
+        const int k = i | (1 << M);
+        Cx<T> x = a[i], y = a[k];
+        if (cm == 0) {
+            a[i] = y;
+            a[k] = x;
+        } else {
+            const bool on = (L.local(i) & cm) == cm;
+            a[i] = on ? y : x;
+            a[k] = on ? x : y;
+        }
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ void op_exchange_any(Cx<T> (&a)[NR], const FusedOp& op, const Layout& L) {
+    if (op.reg2 < 0) {
+        switch (op.reg) {
+        case 0: op_exchange<T, 0>(a, op, L); break;
+        case 1: op_exchange<T, 1>(a, op, L); break;
+#if QM_REG_BITS > 3
+        case 2: op_exchange<T, 2>(a, op, L); break;
+        default: op_exchange<T, 3>(a, op, L); break;
+#else
+        default: op_exchange<T, 2>(a, op, L); break;
+#endif
+        }
+        return;
+    }
+#define QM_XC_CASE(m, mc) \
+    if (op.reg == m && op.reg2 == mc) { op_exchange_rc<T, m, mc>(a, op, L); return; }
+    QM_XC_CASE(0, 1) QM_XC_CASE(0, 2) QM_XC_CASE(1, 0) QM_XC_CASE(1, 2) QM_XC_CASE(2, 0) QM_XC_CASE(2, 1)
+#if QM_REG_BITS > 3
+    QM_XC_CASE(0, 3) QM_XC_CASE(1, 3) QM_XC_CASE(2, 3) QM_XC_CASE(3, 0) QM_XC_CASE(3, 1) QM_XC_CASE(3, 2)
+#endif
+#undef QM_XC_CASE
 }
 
 // SWAP of register bits M1 and M2: exchanges the (M1=1, M2=0) and (M1=0, M2=1) members.
@@ -100,21 +174,39 @@ __device__ __forceinline__ void op_swap(Cx<T> (&a)[NR], const FusedOp& op, const
     for (int i = 0; i < NR; ++i) {
         if (!((i >> M1) & 1) || ((i >> M2) & 1)) continue;
         const int k = i ^ (1 << M1) ^ (1 << M2);
-        if (cm != 0 && (L.local(i) & cm) != cm) continue;
-        Cx<T> x = a[i];
-        a[i] = a[k];
-        a[k] = x;
+        const bool on = (L.local(i) & cm) == cm;
+        Cx<T> x = a[i], y = a[k];
+        a[i] = on ? y : x;
+        a[k] = on ? x : y;
     }
 }
 
 template <typename T>
 __device__ __forceinline__ void op_swap_any(Cx<T> (&a)[NR], const FusedOp& op, const Layout& L) {
+    const int lo = op.reg < op.reg2 ? op.reg : op.reg2, hi = op.reg < op.reg2 ? op.reg2 : op.reg;
 #define QM_SWAP_CASE(m1, m2) \
-    if (op.reg == m1 && op.reg2 == m2) { op_swap<T, m1, m2>(a, op, L); return; }
-    QM_SWAP_CASE(0, 1) QM_SWAP_CASE(0, 2) QM_SWAP_CASE(0, 3) QM_SWAP_CASE(1, 0) QM_SWAP_CASE(1, 2)
-    QM_SWAP_CASE(1, 3) QM_SWAP_CASE(2, 0) QM_SWAP_CASE(2, 1) QM_SWAP_CASE(2, 3) QM_SWAP_CASE(3, 0)
-    QM_SWAP_CASE(3, 1) QM_SWAP_CASE(3, 2)
+    if (lo == m1 && hi == m2) { op_swap<T, m2, m1>(a, op, L); return; }
+    QM_SWAP_CASE(0, 1) QM_SWAP_CASE(0, 2) QM_SWAP_CASE(1, 2)
+#if QM_REG_BITS > 3
+    QM_SWAP_CASE(0, 3) QM_SWAP_CASE(1, 3) QM_SWAP_CASE(2, 3)
+#endif
 #undef QM_SWAP_CASE
+}
+
+// Shared-memory slots of the 2^R registers.  swz() is linear over GF(2) and the base and
+// register bits are disjoint, so slot(base | bits) = swz(base) ^ XOR of swz(register bits):
+// one XOR per register instead of a full swizzle per amplitude.
+template <typename T>
+__device__ __forceinline__ void slots(const Layout& L, uint32_t (&s)[NR]) {
+    uint32_t sp[R];
+#pragma unroll
+    for (int m = 0; m < R; ++m) sp[m] = swz<T>(L.pm[m]);
+    s[0] = swz<T>(L.base);
+#pragma unroll
+    for (int i = 1; i < NR; ++i) {
+        const int low = (i & 1) ? 0 : (i & 2) ? 1 : (i & 4) ? 2 : 3;
+        s[i] = s[i & (i - 1)] ^ sp[low];
+    }
 }
 
 template <typename T>
@@ -123,17 +215,25 @@ __device__ __forceinline__ void op_diag(Cx<T> (&a)[NR], const FusedOp& op, const
     const bool a_one = op.flags & 1, d_one = op.flags & 2;
     const uint32_t cm = op.cmask_local;
     const int lt = op.local;
-    const bool outer_bit = (outer & op.target_outer) != 0;
+    if (lt < 0) {
+        // target outside the block: one phase for the whole CTA
+        const bool bit = (outer & op.target_outer) != 0;
+        if (bit ? d_one : a_one) return;
+        const T pr = bit ? dr : ar, pi = bit ? di : ai;
+#pragma unroll
+        for (int i = 0; i < NR; ++i) {
+            if (cm != 0 && (L.local(i) & cm) != cm) continue;
+            a[i] = cmul<T>(pr, pi, a[i]);
+        }
+        return;
+    }
 #pragma unroll
     for (int i = 0; i < NR; ++i) {
         const uint32_t j = L.local(i);
         if (cm != 0 && (j & cm) != cm) continue;
-        const bool bit = lt >= 0 ? ((j >> lt) & 1u) != 0 : outer_bit;
-        if (bit) {
-            if (!d_one) a[i] = cmul<T>(dr, di, a[i]);
-        } else if (!a_one) {
-            a[i] = cmul<T>(ar, ai, a[i]);
-        }
+        const bool bit = ((j >> lt) & 1u) != 0;
+        if (bit ? d_one : a_one) continue;
+        a[i] = cmul<T>(bit ? dr : ar, bit ? di : ai, a[i]);
     }
 }
 
@@ -142,58 +242,59 @@ __device__ __forceinline__ void op_negate(Cx<T> (&a)[NR], const FusedOp& op, con
     const uint32_t cm = op.cmask_local;
 #pragma unroll
     for (int i = 0; i < NR; ++i) {
-        if ((L.local(i) & cm) != cm) continue;
-        a[i].re = -a[i].re;
-        a[i].im = -a[i].im;
+        const bool on = (L.local(i) & cm) == cm;
+        a[i].re = on ? -a[i].re : a[i].re;
+        a[i].im = on ? -a[i].im : a[i].im;
     }
 }
 
-template <typename T, int K>
-__global__ void __launch_bounds__(1 << (K - R), (sizeof(T) == 8 && K == 12) ? 2 : 1)
-    k_fused(typename Vec2<T>::type* __restrict__ s, const FusedLaunch P, const FusedOp* __restrict__ ops) {
+template <typename T, int K, int MAXOPS>
+__global__ void __launch_bounds__(1 << (K - R), ((sizeof(T) == 8 && K == 12) || (sizeof(T) == 4 && K == 13)) ? 2 : 1)
+    // two CTAs per SM at the default widths: one exchanging with HBM while the other computes
+    k_fused(typename Vec2<T>::type* __restrict__ s, const __grid_constant__ FusedLaunch<MAXOPS> P) {
     using V = typename Vec2<T>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V* tile = reinterpret_cast<V*>(smem_raw);
     const uint32_t t = threadIdx.x;
     const uint32_t outer = deposit(blockIdx.x, P.outer_mask);
 
-    // Canonical layout: the register bits are the top R local bits, so consecutive
-    // threads read consecutive block-local indices (contiguous global runs).
-    uint32_t gthread = outer;
-#pragma unroll
-    for (int b = 0; b < K - R; ++b)
-        if ((t >> b) & 1u) gthread |= 1u << P.q[b];
-    uint32_t greg[R];
-#pragma unroll
-    for (int m = 0; m < R; ++m) greg[m] = 1u << P.q[K - R + m];
-
     Cx<T> a[NR];
+    {
+        const uint32_t g0 = outer | deposit(t, P.thread_in);
 #pragma unroll
-    for (int i = 0; i < NR; ++i) {
-        uint32_t g = gthread;
+        for (int i = 0; i < NR; ++i) {
+            uint32_t g = g0;
 #pragma unroll
-        for (int m = 0; m < R; ++m)
-            if ((i >> m) & 1) g |= greg[m];
-        a[i] = load_amp<T>(s, g);
+            for (int m = 0; m < R; ++m)
+                if ((i >> m) & 1) g |= P.reg_in_g[m];
+            a[i] = load_amp<T>(s, g);
+        }
     }
 
     Layout L;
-    L.base = t;
+    {
+        uint32_t regs = 0;
 #pragma unroll
-    for (int m = 0; m < R; ++m) L.pm[m] = 1u << (K - R + m);
+        for (int m = 0; m < R; ++m) {
+            L.pm[m] = 1u << P.reg_in_l[m];
+            regs |= L.pm[m];
+        }
+        L.base = deposit(t, ((1u << K) - 1u) & ~regs);
+    }
 
-    const int end = P.op_begin + P.op_count;
-    for (int o = P.op_begin; o < end; ++o) {
-        const FusedOp& op = ops[o];
+    for (int o = 0; o < P.op_count; ++o) {
+        const FusedOp& op = P.ops[o];
         const int code = op.code;
         if (code == OP_STAGE) {
+            uint32_t sl[NR];
+            slots<T>(L, sl);
             __syncthreads();
 #pragma unroll
             for (int i = 0; i < NR; ++i) {
                 V v;
                 v.x = a[i].re;
                 v.y = a[i].im;
-                tile[swz<T>(L.local(i))] = v;
+                tile[sl[i]] = v;
             }
             uint32_t regs = 0;
 #pragma unroll
@@ -202,35 +303,27 @@ __global__ void __launch_bounds__(1 << (K - R), (sizeof(T) == 8 && K == 12) ? 2 
                 regs |= L.pm[m];
             }
             L.base = deposit(t, ((1u << K) - 1u) & ~regs);
+            slots<T>(L, sl);
             __syncthreads();
 #pragma unroll
             for (int i = 0; i < NR; ++i) {
-                V v = tile[swz<T>(L.local(i))];
+                V v = tile[sl[i]];
                 a[i] = Cx<T>{v.x, v.y};
             }
             continue;
         }
         if ((outer & op.cmask_outer) != op.cmask_outer) continue;
+        const bool ctrl = op.cmask_local != 0;
         switch (code) {
         case OP_MATRIX:
-        case OP_MATRIX_REAL: {
-            const bool real = code == OP_MATRIX_REAL;
-            switch (op.reg) {
-            case 0: op_matrix<T, 0>(a, op, L, real); break;
-            case 1: op_matrix<T, 1>(a, op, L, real); break;
-            case 2: op_matrix<T, 2>(a, op, L, real); break;
-            default: op_matrix<T, 3>(a, op, L, real); break;
-            }
+            if (ctrl) op_matrix_any<T, false, true>(a, op, L);
+            else op_matrix_any<T, false, false>(a, op, L);
             break;
-        }
-        case OP_EXCHANGE:
-            switch (op.reg) {
-            case 0: op_exchange<T, 0>(a, op, L); break;
-            case 1: op_exchange<T, 1>(a, op, L); break;
-            case 2: op_exchange<T, 2>(a, op, L); break;
-            default: op_exchange<T, 3>(a, op, L); break;
-            }
+        case OP_MATRIX_REAL:
+            if (ctrl) op_matrix_any<T, true, true>(a, op, L);
+            else op_matrix_any<T, true, false>(a, op, L);
             break;
+        case OP_EXCHANGE: op_exchange_any<T>(a, op, L); break;
         case OP_DIAG: op_diag<T>(a, op, L, outer); break;
         case OP_NEGATE: op_negate<T>(a, op, L); break;
         case OP_SWAP: op_swap_any<T>(a, op, L); break;
@@ -238,58 +331,80 @@ __global__ void __launch_bounds__(1 << (K - R), (sizeof(T) == 8 && K == 12) ? 2 
         }
     }
 
-    // The planner ends every pass in the canonical layout.
+    // the planner ends every pass in the store layout
+    const uint32_t g0 = outer | deposit(t, P.thread_out);
 #pragma unroll
     for (int i = 0; i < NR; ++i) {
-        uint32_t g = gthread;
+        uint32_t g = g0;
 #pragma unroll
         for (int m = 0; m < R; ++m)
-            if ((i >> m) & 1) g |= greg[m];
+            if ((i >> m) & 1) g |= P.reg_out_g[m];
         store_amp<T>(s, g, a[i]);
     }
 }
 
-template <typename T, int K>
-cudaError_t launch_k(void* amps, int qubits, const FusedLaunch& L, const FusedOp* d_ops, cudaStream_t st) {
+template <typename T, int K, int MAXOPS>
+cudaError_t launch_k(void* amps, int qubits, const FusedPass& p, const FusedOp* ops, cudaStream_t st) {
     using V = typename Vec2<T>::type;
+    FusedLaunch<MAXOPS> L;
+    const uint32_t all = (1u << qubits) - 1u;
+    L.outer_mask = all & ~p.block_mask;
+    uint32_t reg_in_local = 0, reg_out_local = 0;
+    for (int m = 0; m < R; ++m) {
+        L.reg_in_l[m] = p.reg_in[m];
+        L.pad[m] = 0;
+        L.reg_in_g[m] = 1u << p.q[p.reg_in[m]];
+        L.reg_out_g[m] = 1u << p.q[p.reg_out[m]];
+        reg_in_local |= 1u << p.reg_in[m];
+        reg_out_local |= 1u << p.reg_out[m];
+    }
+    L.thread_in = 0;
+    L.thread_out = 0;
+    for (int b = 0; b < K; ++b) {
+        if (!(reg_in_local & (1u << b))) L.thread_in |= 1u << p.q[b];
+        if (!(reg_out_local & (1u << b))) L.thread_out |= 1u << p.q[b];
+    }
+    L.op_count = p.op_count;
+    for (int i = 0; i < p.op_count; ++i) L.ops[i] = ops[p.op_begin + i];
     const size_t smem = sizeof(V) << K;
     static bool configured = false;
     if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(k_fused<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e =
+            cudaFuncSetAttribute(k_fused<T, K, MAXOPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
         configured = true;
     }
     dim3 grid(1u << (qubits - K));
-    k_fused<T, K><<<grid, 1 << (K - R), smem, st>>>(reinterpret_cast<V*>(amps), L, d_ops);
+    k_fused<T, K, MAXOPS><<<grid, 1 << (K - R), smem, st>>>(reinterpret_cast<V*>(amps), L);
     return cudaGetLastError();
+}
+
+template <typename T, int K>
+cudaError_t launch_sized(void* amps, int qubits, const FusedPass& p, const FusedOp* ops, cudaStream_t st) {
+    if (p.op_count <= kSmallPassOps) return launch_k<T, K, kSmallPassOps>(amps, qubits, p, ops, st);
+    return launch_k<T, K, kMaxPassOps>(amps, qubits, p, ops, st);
 }
 
 }  // namespace
 
-cudaError_t launch_fused(void* amps, int qubits, int precision, const FusedPass& p, const FusedOp* d_ops,
+cudaError_t launch_fused(void* amps, int qubits, int precision, const FusedPass& p, const FusedOp* ops,
                          cudaStream_t st) {
-    FusedLaunch L;
-    uint32_t all = qubits >= 32 ? 0xffffffffu : ((1u << qubits) - 1u);
-    L.outer_mask = all & ~p.block_mask;
-    L.op_begin = p.op_begin;
-    L.op_count = p.op_count;
-    for (int i = 0; i < kMaxBlockQubits; ++i) L.q[i] = i < p.k ? p.q[i] : 0;
-    if (p.k > qubits) return cudaErrorInvalidValue;
+    if (p.k > qubits || p.op_count > kMaxPassOps || p.op_count < 0) return cudaErrorInvalidValue;
     if (precision == QM_FP32) {
         switch (p.k) {
-        case 9: return launch_k<float, 9>(amps, qubits, L, d_ops, st);
-        case 10: return launch_k<float, 10>(amps, qubits, L, d_ops, st);
-        case 11: return launch_k<float, 11>(amps, qubits, L, d_ops, st);
-        case 12: return launch_k<float, 12>(amps, qubits, L, d_ops, st);
-        case 13: return launch_k<float, 13>(amps, qubits, L, d_ops, st);
+        case 9: return launch_sized<float, 9>(amps, qubits, p, ops, st);
+        case 10: return launch_sized<float, 10>(amps, qubits, p, ops, st);
+        case 11: return launch_sized<float, 11>(amps, qubits, p, ops, st);
+        case 12: return launch_sized<float, 12>(amps, qubits, p, ops, st);
+        case 13: return launch_sized<float, 13>(amps, qubits, p, ops, st);
         default: return cudaErrorInvalidValue;
         }
     }
     switch (p.k) {
-    case 9: return launch_k<double, 9>(amps, qubits, L, d_ops, st);
-    case 10: return launch_k<double, 10>(amps, qubits, L, d_ops, st);
-    case 11: return launch_k<double, 11>(amps, qubits, L, d_ops, st);
-    case 12: return launch_k<double, 12>(amps, qubits, L, d_ops, st);
+    case 9: return launch_sized<double, 9>(amps, qubits, p, ops, st);
+    case 10: return launch_sized<double, 10>(amps, qubits, p, ops, st);
+    case 11: return launch_sized<double, 11>(amps, qubits, p, ops, st);
+    case 12: return launch_sized<double, 12>(amps, qubits, p, ops, st);
     default: return cudaErrorInvalidValue;
     }
 }

@@ -46,39 +46,49 @@ DevGate to_dev_gate(const qm_gate& g);
 // that global reads come in contiguous runs), the other qubits are fixed per CTA.
 // Each thread keeps 2^R amplitudes in registers; a stage selects which R local bits
 // are register bits, and every gate of the stage either targets a register bit or is
-// diagonal.  Stage changes go through shared memory.
-constexpr int kRegBits = 4;
+// diagonal.  Stage changes go through shared memory.  The pass's op program travels as
+// a kernel parameter (constant bank), so every op field is a uniform constant load.
+#ifndef QM_REG_BITS
+#define QM_REG_BITS 4
+#endif
+constexpr int kRegBits = QM_REG_BITS;
 constexpr int kMaxBlockQubits = 14;
+constexpr int kMaxPassOps = 352;    // ops per pass: 352 * 88 B + header <= 32 KB of parameters
+constexpr int kSmallPassOps = 48;   // launch variant for short programs (smaller parameter copy)
+constexpr int kMaxPassGates = 170;  // gates absorbed per pass (stage changes add at most gates + 2)
 
-enum OpCode : int32_t {
-    OP_STAGE = 0,      // new register layout: reg_pos[0..R) local bit positions
-    OP_MATRIX = 1,     // complex 2x2 on register bit `reg`
-    OP_MATRIX_REAL = 2,// real 2x2 (imaginary parts all zero)
-    OP_EXCHANGE = 3,   // X on register bit `reg`
-    OP_DIAG = 4,       // diagonal: a on bit-zero, d on bit-one of local bit `local` (or outer bit)
-    OP_NEGATE = 5,     // amplitude *= -1 where all of (local_mask | target) set: CZ, Z
-    OP_SWAP = 6,       // exchange register bits `reg` and `reg2`
+enum OpCode : uint8_t {
+    OP_STAGE = 0,       // new register layout: reg_pos[0..R) local bit positions
+    OP_MATRIX = 1,      // complex 2x2 on register bit `reg`
+    OP_MATRIX_REAL = 2, // real 2x2 (imaginary parts all zero)
+    OP_EXCHANGE = 3,    // X on register bit `reg`
+    OP_DIAG = 4,        // diagonal: a on bit-zero, d on bit-one of local bit `local` (or outer bit)
+    OP_NEGATE = 5,      // amplitude *= -1 where all of (cmask_local, cmask_outer) bits are set: CZ, Z
+    OP_SWAP = 6,        // exchange register bits `reg` and `reg2`
 };
 
-struct FusedOp {
-    int32_t code;
-    int32_t reg;            // register bit (0..R) of the target, or -1
-    int32_t reg2;           // second register bit for OP_SWAP
-    int32_t local;          // local bit of a diagonal target, -1 when the target is outside the block
-    uint32_t cmask_local;   // controls inside the block, as local-index bits
+struct FusedOp {            // 88 bytes
+    uint8_t code;
+    int8_t reg;             // register bit (0..R) of the target, or -1
+    int8_t reg2;            // second register bit for OP_SWAP; control register bit for OP_EXCHANGE (-1: none)
+    int8_t local;           // local bit of a diagonal target, -1 when the target is outside the block
+    int8_t reg_pos[4];      // OP_STAGE: local bit positions of the register bits (ascending; kRegBits used)
+    uint16_t cmask_local;   // controls inside the block, as local-index bits
+    uint16_t flags;         // bit0: a == 1, bit1: d == 1 (diagonal)
     uint32_t cmask_outer;   // controls outside the block, as global-index bits
     uint32_t target_outer;  // outer target bit of a diagonal (global), 0 when local
-    int32_t flags;          // bit0: a == 1, bit1: d == 1 (diagonal)
-    int32_t reg_pos[kRegBits];  // OP_STAGE: local bit positions of the register bits
+    uint32_t reserved;
     double coef[8];         // a, b, c, d as (re, im)
 };
 
-struct FusedPass {
+struct FusedPass {                  // 84 bytes
     int32_t k;                      // block qubits
     int32_t op_begin, op_count;     // range in the plan's op array
     int32_t q[kMaxBlockQubits];     // block qubits, ascending
     uint32_t block_mask;            // OR of 1<<q[i]
-    int32_t stages;                 // number of register layouts (>= 1)
+    int32_t stages;                 // number of register layouts
+    int8_t reg_in[4];               // local register bits of the load layout (ascending; kRegBits used)
+    int8_t reg_out[4];              // local register bits of the store layout (ascending; kRegBits used)
 };
 
 struct Plan {
@@ -88,7 +98,6 @@ struct Plan {
     std::vector<DevGate> gates;     // per-gate path
     std::vector<FusedPass> passes;  // fused path
     std::vector<FusedOp> ops;
-    FusedOp* d_ops = nullptr;       // device copy of ops
     int64_t planned_bytes = 0;
     int32_t launches = 0;
 };
@@ -100,7 +109,7 @@ int default_block_qubits(int qubits, int precision);
 
 // ---------------------------------------------------------------- launchers (qm_kernels.cu)
 cudaError_t launch_gate(void* amps, int qubits, int precision, const DevGate& g, cudaStream_t s);
-cudaError_t launch_fused(void* amps, int qubits, int precision, const FusedPass& p, const FusedOp* d_ops,
+cudaError_t launch_fused(void* amps, int qubits, int precision, const FusedPass& p, const FusedOp* ops,
                          cudaStream_t s);
 cudaError_t launch_reset(void* amps, int qubits, int precision, cudaStream_t s);
 cudaError_t launch_convert_from_f64(void* dst_f32, const double* src_f64, int64_t n, cudaStream_t s);

@@ -399,7 +399,10 @@ __global__ void k_search(const typename Vec2<T>::type* __restrict__ s, const dou
                 double at = __shfl_sync(0xffffffffu, cum, l);
                 double before = __shfl_sync(0xffffffffu, cum - p, l);
                 found = begin + off + l;
-                ambiguous = (fabs(at - t) <= margin) || (fabs(t - before) <= margin);
+                // the reference's CDF could still be <= t here (it would pick a later index),
+                // or could already exceed t one supported index earlier; with no mass before
+                // this index there is no earlier outcome to pick
+                ambiguous = (at - t <= margin) || (before > 0 && t - before <= margin);
                 break;
             }
             running = __shfl_sync(0xffffffffu, cum, 31);

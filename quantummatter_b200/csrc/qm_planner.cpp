@@ -139,7 +139,7 @@ bool plan_fused(const std::vector<qm_gate>& gates, int qubits, int precision, in
         uint32_t bx = 0, bz = 0;
         std::vector<GInfo> absorbed, rest;
         for (const GInfo& g : remaining) {
-            if (!blocked(g, bx, bz)) {
+            if ((int)absorbed.size() < kMaxPassGates && !blocked(g, bx, bz)) {
                 uint32_t nq = Q | g.need;
                 if (popc(nq) <= k) {
                     Q = nq;
@@ -155,7 +155,12 @@ bool plan_fused(const std::vector<qm_gate>& gates, int qubits, int precision, in
             error = "planner made no progress";
             return false;
         }
-        // fill the block to k qubits with the lowest unused qubits
+        // fill the block to k qubits: qubits the remaining gates need first, then the lowest
+        for (const GInfo& g : rest) {
+            if (popc(Q) >= k) break;
+            uint32_t extra = g.need & ~Q;
+            if (extra && popc(Q | extra) <= k) Q |= extra;
+        }
         for (int q = 0; q < qubits && popc(Q) < k; ++q) Q |= 1u << q;
 
         FusedPass pass{};
@@ -170,55 +175,102 @@ bool plan_fused(const std::vector<qm_gate>& gates, int qubits, int precision, in
                 pass.q[nb++] = q;
             }
         pass.op_begin = (int32_t)plan.ops.size();
-
-        // stage planning inside the pass (capacity R register bits)
-        const uint32_t canonical = ((1u << kRegBits) - 1u) << (k - kRegBits);  // local bits
-        uint32_t layout = canonical;                                       // current local register bits
-        std::vector<GInfo> pending = absorbed;
-        int stages = 0;
-        while (!pending.empty()) {
-            uint32_t P = 0;  // global qubits needed in registers
-            uint32_t sbx = 0, sbz = 0;
-            std::vector<GInfo> stage_gates, later;
-            for (const GInfo& g : pending) {
-                if (!blocked(g, sbx, sbz)) {
-                    if (g.diag) {
-                        stage_gates.push_back(g);
-                        continue;
-                    }
-                    uint32_t np = P | g.need;
-                    if (popc(np) <= kRegBits) {
-                        P = np;
-                        stage_gates.push_back(g);
-                        continue;
-                    }
-                }
-                later.push_back(g);
-                sbx |= g.xmask;
-                sbz |= g.zmask;
-            }
-            // local register mask: needed qubits, then the current layout's bits (no data
-            // movement when it already fits), then the highest local bits
-            uint32_t Pl = 0;
+        auto to_local = [&](uint32_t global) {
+            uint32_t l = 0;
             for (int q = 0; q < qubits; ++q)
-                if (P & (1u << q)) Pl |= 1u << local_of[q];
-            uint32_t new_layout;
-            if ((Pl & ~layout) == 0) {
-                new_layout = layout;
-            } else {
-                new_layout = Pl;
-                for (int b = k - 1; b >= 0 && popc(new_layout) < kRegBits; --b)
-                    if ((layout & (1u << b)) && !(new_layout & (1u << b))) new_layout |= 1u << b;
-                for (int b = k - 1; b >= 0 && popc(new_layout) < kRegBits; --b) new_layout |= 1u << b;
+                if (global & (1u << q)) l |= 1u << local_of[q];
+            return l;
+        };
+
+        // 1) split the pass into stages: each stage holds gates whose register needs fit in
+        //    kRegBits qubits, in commutation-respecting order
+        std::vector<std::vector<GInfo>> stage_gates;
+        std::vector<uint32_t> stage_need;  // local bits
+        std::vector<uint32_t> stage_soft;  // local bits worth holding (controls of X gates)
+        {
+            std::vector<GInfo> pending = absorbed;
+            while (!pending.empty()) {
+                uint32_t P = 0, sbx = 0, sbz = 0;
+                std::vector<GInfo> mine, later;
+                for (const GInfo& g : pending) {
+                    if (!blocked(g, sbx, sbz)) {
+                        if (g.diag) {
+                            mine.push_back(g);
+                            continue;
+                        }
+                        uint32_t np = P | g.need;
+                        if (popc(np) <= kRegBits) {
+                            P = np;
+                            mine.push_back(g);
+                            continue;
+                        }
+                    }
+                    later.push_back(g);
+                    sbx |= g.xmask;
+                    sbz |= g.zmask;
+                }
+                // controls of X gates are worth holding in registers too: the X then becomes
+                // a fixed register permutation
+                uint32_t soft = 0;
+                for (const GInfo& g : mine)
+                    if (g.g.kernel == QM_KERNEL_EXCHANGE) soft |= g.g.control_mask & Q;
+                stage_gates.push_back(mine);
+                stage_need.push_back(to_local(P));
+                stage_soft.push_back(to_local(soft) & ~((1u << low_bits) - 1u));
+                pending.swap(later);
             }
-            if (new_layout != layout) {
-                FusedOp st{};
-                st.code = OP_STAGE;
-                int m = 0;
-                for (int b = 0; b < k; ++b)
-                    if (new_layout & (1u << b)) st.reg_pos[m++] = b;
-                plan.ops.push_back(st);
-                layout = new_layout;
+        }
+        // 2) register layouts: keep the current layout when it already covers a stage's
+        //    needs; otherwise take the needs, then the next stages' needs (so the following
+        //    stage may not need a change), then the current layout, then the highest bits.
+        //    Low local bits (the coalescing run) are never used as filler.
+        const uint32_t low_local = (1u << low_bits) - 1u;
+        const uint32_t canonical = ((1u << kRegBits) - 1u) << (k - kRegBits);
+        auto fill = [&](uint32_t need, size_t from, uint32_t current) {
+            uint32_t l = need;
+            if (from >= 1) {
+                uint32_t soft = stage_soft[from - 1] & ~l;
+                for (int b = 0; b < k && popc(l) < kRegBits; ++b)
+                    if (soft & (1u << b)) l |= 1u << b;
+            }
+            for (size_t s = from; s < stage_need.size() && popc(l) < kRegBits; ++s) {
+                uint32_t extra = stage_need[s] & ~l & ~low_local;
+                for (int b = 0; b < k && popc(l) < kRegBits; ++b)
+                    if (extra & (1u << b)) l |= 1u << b;
+            }
+            for (int b = k - 1; b >= 0 && popc(l) < kRegBits; --b)
+                if ((current & (1u << b)) && !(low_local & (1u << b))) l |= 1u << b;
+            for (int b = k - 1; b >= 0 && popc(l) < kRegBits; --b)
+                if (!(low_local & (1u << b))) l |= 1u << b;
+            return l;
+        };
+        auto emit_stage = [&](uint32_t layout) {
+            FusedOp st{};
+            st.code = OP_STAGE;
+            st.reg = st.reg2 = st.local = -1;
+            int m = 0;
+            for (int b = 0; b < k; ++b)
+                if (layout & (1u << b)) st.reg_pos[m++] = (int8_t)b;
+            plan.ops.push_back(st);
+        };
+        auto set_regs = [&](int8_t* dst, uint32_t layout) {
+            int m = 0;
+            for (int b = 0; b < k; ++b)
+                if (layout & (1u << b)) dst[m++] = (int8_t)b;
+        };
+        uint32_t layout = fill(stage_need.empty() ? 0 : stage_need[0], 1, canonical);
+        int stages = 1;
+        if (layout & low_local) {
+            set_regs(pass.reg_in, canonical);
+            emit_stage(layout);
+            ++stages;
+        } else {
+            set_regs(pass.reg_in, layout);
+        }
+        for (size_t si = 0; si < stage_gates.size(); ++si) {
+            if ((stage_need[si] & ~layout) != 0) {
+                layout = fill(stage_need[si], si + 1, layout);
+                emit_stage(layout);
                 ++stages;
             }
             int reg_of_local[32];
@@ -228,14 +280,14 @@ bool plan_fused(const std::vector<qm_gate>& gates, int qubits, int precision, in
                 for (int b = 0; b < k; ++b)
                     if (layout & (1u << b)) reg_of_local[b] = m++;
             }
-            for (const GInfo& gi : stage_gates) {
+            for (const GInfo& gi : stage_gates[si]) {
                 const qm_gate& g = gi.g;
                 FusedOp op{};
                 op.reg = op.reg2 = -1;
                 op.local = -1;
                 for (int q = 0; q < qubits; ++q) {
                     if (!(g.control_mask & (1u << q))) continue;
-                    if (local_of[q] >= 0) op.cmask_local |= 1u << local_of[q];
+                    if (local_of[q] >= 0) op.cmask_local |= (uint16_t)(1u << local_of[q]);
                     else op.cmask_outer |= 1u << q;
                 }
                 std::memcpy(&op.coef[0], g.a, 16);
@@ -247,25 +299,28 @@ bool plan_fused(const std::vector<qm_gate>& gates, int qubits, int precision, in
                     int lt = local_of[g.target];
                     if (a1 && is_exact(g.d, -1.0, 0.0)) {
                         op.code = OP_NEGATE;
-                        if (lt >= 0) op.cmask_local |= 1u << lt;
+                        if (lt >= 0) op.cmask_local |= (uint16_t)(1u << lt);
                         else op.cmask_outer |= 1u << g.target;
                     } else {
                         op.code = OP_DIAG;
-                        op.local = lt;
+                        op.local = (int8_t)lt;
                         op.target_outer = lt >= 0 ? 0u : (1u << g.target);
-                        op.flags = (a1 ? 1 : 0) | (d1 ? 2 : 0);
+                        op.flags = (uint16_t)((a1 ? 1 : 0) | (d1 ? 2 : 0));
                     }
                 } else if (g.kernel == QM_KERNEL_EXCHANGE) {
                     op.code = OP_EXCHANGE;
-                    op.reg = reg_of_local[local_of[g.target]];
+                    op.reg = (int8_t)reg_of_local[local_of[g.target]];
+                    for (int q = 0; q < qubits && op.reg2 < 0; ++q)
+                        if ((g.control_mask & (1u << q)) && local_of[q] >= 0 && reg_of_local[local_of[q]] >= 0)
+                            op.reg2 = (int8_t)reg_of_local[local_of[q]];
                 } else if (g.kernel == QM_KERNEL_SWAP) {
                     op.code = OP_SWAP;
-                    op.reg = reg_of_local[local_of[g.target]];
-                    op.reg2 = reg_of_local[local_of[g.swap_control]];
+                    op.reg = (int8_t)reg_of_local[local_of[g.target]];
+                    op.reg2 = (int8_t)reg_of_local[local_of[g.swap_control]];
                 } else {
                     bool real = g.a[1] == 0 && g.b[1] == 0 && g.c[1] == 0 && g.d[1] == 0;
                     op.code = real ? OP_MATRIX_REAL : OP_MATRIX;
-                    op.reg = reg_of_local[local_of[g.target]];
+                    op.reg = (int8_t)reg_of_local[local_of[g.target]];
                 }
                 if ((op.code == OP_MATRIX || op.code == OP_MATRIX_REAL || op.code == OP_EXCHANGE) && op.reg < 0) {
                     error = "planner placed a gate outside the register layout";
@@ -277,18 +332,19 @@ bool plan_fused(const std::vector<qm_gate>& gates, int qubits, int precision, in
                 }
                 plan.ops.push_back(op);
             }
-            pending.swap(later);
         }
-        if (layout != canonical) {
-            FusedOp st{};
-            st.code = OP_STAGE;
-            int m = 0;
-            for (int b = 0; b < k; ++b)
-                if (canonical & (1u << b)) st.reg_pos[m++] = b;
-            plan.ops.push_back(st);
+        if (layout & low_local) {
+            emit_stage(canonical);
             ++stages;
+            set_regs(pass.reg_out, canonical);
+        } else {
+            set_regs(pass.reg_out, layout);
         }
         pass.op_count = (int32_t)plan.ops.size() - pass.op_begin;
+        if (pass.op_count > kMaxPassOps) {
+            error = "pass program exceeds the kernel-parameter capacity";
+            return false;
+        }
         pass.stages = stages;
         plan.passes.push_back(pass);
         plan.planned_bytes += 2 * n * elem;

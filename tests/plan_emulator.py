@@ -50,8 +50,8 @@ def emulate(state: np.ndarray, qubits: int, passes, ops, reg_bits: int = 4) -> n
         local = np.arange(1 << k, dtype=np.int64)
         idx = outer[:, None] | deposit(local, p.block_mask)[None, :]
         blk = s[idx]
-        canonical = list(range(k - reg_bits, k))
-        layout = canonical
+        layout = list(p.reg_in)
+        assert all(b >= 3 for b in layout), "the load layout keeps the lowest qubits on thread bits"
         for op in ops[p.op_begin:p.op_begin + p.op_count]:
             if op.code == OP_STAGE:
                 layout = list(op.reg_pos)
@@ -91,6 +91,7 @@ def emulate(state: np.ndarray, qubits: int, passes, ops, reg_bits: int = 4) -> n
                 blk = np.where(mask, blk * phase, blk)
             else:
                 raise AssertionError(f"unknown op {op.code}")
-        assert layout == canonical, "a pass must end in the canonical layout"
+        assert layout == list(p.reg_out), "a pass must end in its store layout"
+        assert all(b >= 3 for b in layout), "the store layout keeps the lowest qubits on thread bits"
         s[idx] = blk
     return s

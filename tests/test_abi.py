@@ -41,8 +41,8 @@ def test_struct_layouts_match_the_header():
     assert C.sizeof(_lib.Operation) == 88
     assert C.sizeof(_lib.Gate) == 80
     assert C.sizeof(_lib.PauliTermC) == 24
-    assert C.sizeof(_lib.FusedOpInfo) == 112
-    assert C.sizeof(_lib.FusedPassInfo) == 76
+    assert C.sizeof(_lib.FusedOpInfo) == 88
+    assert C.sizeof(_lib.FusedPassInfo) == 84
     assert C.sizeof(_lib.Options) == 56
 
 
