@@ -282,6 +282,57 @@ int32_t qm_measure_all(qm_state* state, double u, int64_t* outcome, int32_t* amb
 int32_t qm_sample(qm_state* state, const double* draws, int32_t shots, int64_t* outcomes,
                   int32_t* ambiguous);
 
+/* ---------------------------------------------------------------- batches */
+
+/* A device batch of `capacity` equally sized states (qubits in [9,30]).  All states of one
+ * execution share a gate structure; gates with a nonnegative slot read their coefficients
+ * (a, b, c, d as 8 doubles) per state from `table` ([states][slot_count][8]).  This is the
+ * engine behind batched trajectories, parameter-shift circuits and served requests. */
+typedef struct qm_batch qm_batch;
+int32_t qm_batch_create(qm_context* context, int32_t qubits, int32_t precision, int32_t capacity, qm_batch** batch);
+int32_t qm_batch_destroy(qm_batch* batch);
+int32_t qm_batch_reset(qm_batch* batch, int32_t states);          /* first `states` states to |0...0> */
+/* Copies one state to (upload = 0) or from (upload != 0) a host complex128 array. */
+int32_t qm_batch_state(qm_batch* batch, int32_t index, double* amplitudes, int64_t length, int32_t upload);
+int32_t qm_batch_execute(qm_batch* batch, int32_t states, const qm_gate* gates, const int32_t* slots, int32_t count,
+                         const double* table, int32_t slot_count, int32_t fusion_width);
+/* values[state][term] = <P_t> / mass (coefficients ignored), masses[state] (may be NULL). */
+int32_t qm_batch_expectation(qm_batch* batch, int32_t states, const qm_pauli_term* terms, int32_t count,
+                             double* values, double* masses);
+
+/* ---------------------------------------------------------------- variational */
+
+/* One operation of a ParameterizedCircuit template (src/QuantumMatter.Core/Variational/
+ * ParameterizedCircuit.cs:98): a constant gate (parameter = -1) or an uncontrolled Rx/Ry/Rz
+ * whose angle is parameters[parameter]. */
+typedef struct qm_template_op {
+    qm_operation operation;
+    int32_t parameter;
+    int32_t reserved;
+} qm_template_op;            /* 96 bytes */
+
+typedef struct qm_vqe_stats {
+    int64_t circuits;         /* circuits evaluated: vectors * (1 + 2 * rotations) with gradients */
+    int32_t waves;            /* batch waves (CUDA-graph replays for full waves) */
+    int32_t batch_states;
+    int32_t passes_per_circuit;
+    int32_t tile_passes;
+    double device_seconds;
+    double wall_seconds;
+} qm_vqe_stats;
+
+/* VariationalEnergyEvaluator.Evaluate / EvaluateWithGradient
+ * (src/QuantumMatter.Application/Variational/VariationalEnergyEvaluator.cs:23-86) for `vectors`
+ * parameter vectors at once: parameters[vector][parameter_count] -> energies[vector] and, when
+ * with_gradient != 0, gradients[vector][parameter_count] by the occurrence-wise +-pi/2
+ * parameter-shift rule with termwise differencing and Neumaier accumulation.  Every base and
+ * shifted circuit runs as a state of device batches (waves sized by the device budget).
+ * stats may be NULL. */
+int32_t qm_vqe_evaluate(qm_context* context, int32_t qubits, int32_t precision, const qm_template_op* operations,
+                        int32_t operation_count, int32_t parameter_count, const qm_pauli_term* terms,
+                        int32_t term_count, const double* parameters, int32_t vectors, int32_t with_gradient,
+                        double* energies, double* gradients, qm_vqe_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -66,6 +66,16 @@ class FusedOpInfo(C.Structure):
                 ("coef", C.c_double * 8)]
 
 
+class TemplateOp(C.Structure):
+    _fields_ = [("operation", Operation), ("parameter", C.c_int32), ("reserved", C.c_int32)]
+
+
+class VqeStats(C.Structure):
+    _fields_ = [("circuits", C.c_int64), ("waves", C.c_int32), ("batch_states", C.c_int32),
+                ("passes_per_circuit", C.c_int32), ("tile_passes", C.c_int32), ("device_seconds", C.c_double),
+                ("wall_seconds", C.c_double)]
+
+
 NEXT_DOUBLE_FN = C.CFUNCTYPE(C.c_double, C.c_void_p)
 
 P = C.c_void_p
@@ -109,6 +119,14 @@ SIGNATURES = {
     "qm_expectation_energy": (I32, [P, C.POINTER(PauliTermC), I32, DP]),
     "qm_measure_all": (I32, [P, C.c_double, I64P, I32P]),
     "qm_sample": (I32, [P, DP, I32, I64P, I32P]),
+    "qm_batch_create": (I32, [P, I32, I32, I32, C.POINTER(P)]),
+    "qm_batch_destroy": (I32, [P]),
+    "qm_batch_reset": (I32, [P, I32]),
+    "qm_batch_state": (I32, [P, I32, P, I64, I32]),
+    "qm_batch_execute": (I32, [P, I32, C.POINTER(Gate), I32P, I32, DP, I32, I32]),
+    "qm_batch_expectation": (I32, [P, I32, C.POINTER(PauliTermC), I32, DP, DP]),
+    "qm_vqe_evaluate": (I32, [P, I32, I32, C.POINTER(TemplateOp), I32, I32, C.POINTER(PauliTermC), I32, DP, I32, I32,
+                              DP, DP, C.POINTER(VqeStats)]),
 }
 
 _lock = threading.Lock()

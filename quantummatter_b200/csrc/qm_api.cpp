@@ -251,7 +251,7 @@ int32_t run_plan(qm_context* ctx, const Plan& plan, void* amps, const volatile i
         }
     } else {
         for (const FusedPass& p : plan.passes) {
-            QM_CUDA(launch_fused(amps, plan.qubits, plan.precision, p, plan.ops.data(), ctx->stream));
+            QM_CUDA(launch_fused(amps, plan.qubits, plan.precision, p, plan.ops.data(), nullptr, ctx->stream));
             int32_t rc = chunk_boundary();
             if (rc) return rc;
         }
@@ -889,9 +889,33 @@ int32_t validate_terms(const qm_pauli_term* terms, int32_t count, int qubits) {
     return QM_OK;
 }
 
-// Raw term sums and mass into host arrays (raw[count], *mass).
+// Raw term sums and mass into host arrays (raw[count], *mass).  States of 9 or more qubits use
+// the tiled kernel (a few reads of the state for the whole term list); smaller ones run one
+// pass per distinct flip mask.
 int32_t device_expectation(qm_state* st, const qm_pauli_term* terms, int32_t count, double* raw, double* mass) {
     qm_context* ctx = st->ctx;
+    TilePlan tp;
+    std::string err;
+    if (st->qubits >= 9 && plan_tiles(st->qubits, st->precision, terms, count, tp, err)) {
+        const size_t cells = (size_t)tp.rows_per_state * tp.columns;
+        int32_t rc = ensure_scratch(ctx, sizeof(double) * (cells + tp.columns));
+        if (rc) return rc;
+        rc = ensure_host_scratch(ctx, sizeof(double) * tp.columns);
+        if (rc) return rc;
+        double* partial = static_cast<double*>(ctx->scratch);
+        double* out = partial + cells;
+        QM_CUDA(cudaMemsetAsync(partial, 0, sizeof(double) * cells, ctx->stream));
+        for (const TilePass& p : tp.passes)
+            QM_CUDA(launch_expect_tile(st->amps, st->qubits, st->precision, p, tp.terms.data(), 1, 0, partial,
+                                       tp.columns, tp.rows_per_state, tp.mass_column, ctx->stream));
+        QM_CUDA(launch_finish_batched(partial, 1, tp.rows_per_state, tp.columns, out, ctx->stream));
+        QM_CUDA(cudaMemcpyAsync(ctx->host_scratch, out, sizeof(double) * tp.columns, cudaMemcpyDeviceToHost,
+                                ctx->stream));
+        QM_CUDA(cudaStreamSynchronize(ctx->stream));
+        for (int32_t i = 0; i < count; ++i) raw[i] = ctx->host_scratch[i];
+        *mass = ctx->host_scratch[tp.mass_column];
+        return QM_OK;
+    }
     std::vector<DevPauli> dev((size_t)count);
     for (int32_t i = 0; i < count; ++i)
         dev[(size_t)i] = DevPauli{terms[i].flip_mask, terms[i].sign_mask, terms[i].y_count & 3, 0};

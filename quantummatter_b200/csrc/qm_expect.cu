@@ -1,0 +1,235 @@
+// qm_expect.cu -- tiled Pauli-sum expectation for batches of states (sm_100a).
+//
+// StateVector.ExpectationValue (StateVector.Observations.cs:107-141) evaluates one term per
+// pass over the state.  Here a CTA stages a block of 2^K amplitudes in shared memory (the
+// block's qubits are a "tile": the lowest qubits plus a window chosen so that the flip masks
+// of the assigned terms lie inside it) and evaluates every assigned term against it:
+// conj(psi[j ^ F]) psi[j] with the Y phase and the Z-sign parity of the global index, in
+// FP64.  A Hamiltonian whose flip masks fit in a few windows costs a few reads of the state
+// instead of one per term.  Sums are deterministic: thread, warp tree, fixed warp order, and
+// a fixed-order column sum over CTAs.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "qm_device.cuh"
+#include "qm_internal.h"
+
+namespace qm {
+
+namespace {
+
+constexpr int R = kRegBits;
+constexpr int NR = 1 << R;
+
+template <int MAXT>
+struct TileLaunch {
+    uint32_t outer_mask;      // qubits outside the tile
+    uint32_t thread_mask;     // global bits carried by the thread index (local bits 0..K-R-1)
+    uint32_t reg_g[R];        // global bits of the register index (local bits K-R..K-1)
+    int32_t terms;
+    int32_t with_mass;
+    int32_t columns;          // row width of the partial table
+    int32_t mass_column;
+    int32_t row_offset;       // first partial row of this tile pass
+    int32_t rows_per_state;
+    uint64_t state_stride;
+    double* partials;         // [states][rows_per_state][columns]
+    TileTerm t[MAXT];
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int d = 16; d > 0; d >>= 1) v += __shfl_down_sync(0xffffffffu, v, d);
+    return v;
+}
+
+template <typename T, int K, int MAXT>
+__global__ void __launch_bounds__(1 << (K - R))
+    k_expect_tile(const typename Vec2<T>::type* __restrict__ s, const __grid_constant__ TileLaunch<MAXT> P) {
+    using V = typename Vec2<T>::type;
+    constexpr int NT = 1 << (K - R);
+    constexpr int WARPS = NT / 32;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V* tile = reinterpret_cast<V*>(smem_raw);
+    double* red = reinterpret_cast<double*>(smem_raw + (sizeof(V) << K));  // [WARPS][terms + 1]
+    const uint32_t t = threadIdx.x;
+    const int warp = t >> 5, lane = t & 31;
+    s += (size_t)blockIdx.y * P.state_stride;
+    const uint32_t outer = deposit(blockIdx.x, P.outer_mask);
+    const uint32_t g0 = outer | deposit(t, P.thread_mask);
+
+    Cx<T> a[NR];
+    uint32_t g[NR];
+#pragma unroll
+    for (int i = 0; i < NR; ++i) {
+        uint32_t gi = g0;
+#pragma unroll
+        for (int m = 0; m < R; ++m)
+            if ((i >> m) & 1) gi |= P.reg_g[m];
+        g[i] = gi;
+        a[i] = load_amp<T>(s, gi);
+        V v;
+        v.x = a[i].re;
+        v.y = a[i].im;
+        tile[t | ((uint32_t)i << (K - R))] = v;
+    }
+    __syncthreads();
+
+    for (int k = 0; k < P.terms; ++k) {
+        const TileTerm term = P.t[k];
+        double acc = 0.0;
+#pragma unroll
+        for (int i = 0; i < NR; ++i) {
+            const double ar = a[i].re, ai = a[i].im;
+            double ore, oim;
+            if (term.flip_local == 0) {
+                ore = ar * ar + ai * ai;
+                oim = 0.0;
+            } else {
+                const V b = tile[(t | ((uint32_t)i << (K - R))) ^ term.flip_local];
+                const double br = b.x, bi = b.y;
+                ore = br * ar + bi * ai;
+                oim = br * ai - bi * ar;
+            }
+            double c;
+            switch (term.phase) {
+            case 0: c = ore; break;
+            case 1: c = -oim; break;
+            case 2: c = -ore; break;
+            default: c = oim; break;
+            }
+            acc += (__popc(g[i] & term.sign) & 1) ? -c : c;
+        }
+        acc = warp_sum(acc);
+        if (lane == 0) red[warp * (P.terms + 1) + k] = acc;
+    }
+    if (P.with_mass) {
+        double acc = 0.0;
+#pragma unroll
+        for (int i = 0; i < NR; ++i) acc += (double)a[i].re * a[i].re + (double)a[i].im * a[i].im;
+        acc = warp_sum(acc);
+        if (lane == 0) red[warp * (P.terms + 1) + P.terms] = acc;
+    }
+    __syncthreads();
+    const size_t row = (size_t)blockIdx.y * P.rows_per_state + P.row_offset + blockIdx.x;
+    for (int k = t; k < P.terms + (P.with_mass ? 1 : 0); k += NT) {
+        double sum = 0.0;
+        for (int w = 0; w < WARPS; ++w) sum += red[w * (P.terms + 1) + k];
+        const int col = k < P.terms ? P.t[k].column : P.mass_column;
+        P.partials[row * P.columns + col] = sum;
+    }
+}
+
+template <typename T, int K, int MAXT>
+cudaError_t launch_tile_k(const void* amps, int qubits, const TilePass& tp, const TileTerm* terms, int states,
+                          uint64_t state_stride, double* partials, int columns, int rows_per_state, int mass_column,
+                          cudaStream_t st) {
+    using V = typename Vec2<T>::type;
+    TileLaunch<MAXT> L;
+    const uint32_t all = (1u << qubits) - 1u;
+    L.outer_mask = all & ~tp.block_mask;
+    L.thread_mask = 0;
+    for (int b = 0; b < K - R; ++b) L.thread_mask |= 1u << tp.q[b];
+    for (int m = 0; m < R; ++m) L.reg_g[m] = 1u << tp.q[K - R + m];
+    L.terms = tp.term_count;
+    L.with_mass = tp.with_mass;
+    L.columns = columns;
+    L.mass_column = mass_column;
+    L.row_offset = tp.row_offset;
+    L.rows_per_state = rows_per_state;
+    L.state_stride = state_stride;
+    L.partials = partials;
+    for (int i = 0; i < tp.term_count; ++i) L.t[i] = terms[tp.term_begin + i];
+    const size_t smem = (sizeof(V) << K) + sizeof(double) * (size_t)((1 << (K - R)) / 32) * (tp.term_count + 1);
+    static bool configured = false;
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(k_expect_tile<T, K, MAXT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)((sizeof(V) << K) + sizeof(double) * ((1 << (K - R)) / 32) * (MAXT + 1)));
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    dim3 grid(1u << (qubits - K), (unsigned)states);
+    k_expect_tile<T, K, MAXT><<<grid, 1 << (K - R), smem, st>>>(reinterpret_cast<const V*>(amps), L);
+    return cudaGetLastError();
+}
+
+template <typename T, int K>
+cudaError_t launch_tile_sized(const void* amps, int qubits, const TilePass& tp, const TileTerm* terms, int states,
+                              uint64_t stride, double* partials, int columns, int rows, int mass_column,
+                              cudaStream_t st) {
+    if (tp.term_count <= 32)
+        return launch_tile_k<T, K, 32>(amps, qubits, tp, terms, states, stride, partials, columns, rows, mass_column, st);
+    return launch_tile_k<T, K, kTileMaxTerms>(amps, qubits, tp, terms, states, stride, partials, columns, rows,
+                                              mass_column, st);
+}
+
+// Column sums per state of a [states][rows][columns] table: one warp per (state, column).
+__global__ void k_finish_batched(const double* __restrict__ partials, int rows, int columns, double* out) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= columns) return;
+    const size_t base = (size_t)blockIdx.y * rows * columns;
+    KSum acc{0, 0};
+    for (int r = lane; r < rows; r += 32) acc.add(partials[base + (size_t)r * columns + warp]);
+    for (int d = 16; d > 0; d >>= 1) acc.merge(shfl_down_ksum(acc, d));
+    if (lane == 0) out[(size_t)blockIdx.y * columns + warp] = acc.value();
+}
+
+template <typename T>
+__global__ void k_reset_batched(typename Vec2<T>::type* s, uint64_t per_state, uint64_t total) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (; i < total; i += stride) {
+        typename Vec2<T>::type v;
+        v.x = (i % per_state) == 0 ? (T)1 : (T)0;
+        v.y = (T)0;
+        s[i] = v;
+    }
+}
+
+}  // namespace
+
+int tile_block_qubits(int qubits, int precision) {
+    int k = precision == QM_FP32 ? 12 : 11;  // leaves room for the per-warp term sums in shared memory
+    return k < qubits ? k : qubits;
+}
+
+cudaError_t launch_expect_tile(const void* amps, int qubits, int precision, const TilePass& tp, const TileTerm* terms,
+                               int states, uint64_t state_stride, double* partials, int columns, int rows_per_state,
+                               int mass_column, cudaStream_t st) {
+    if (tp.term_count > kTileMaxTerms || tp.term_count < 0 || states < 1 || states > 65535)
+        return cudaErrorInvalidValue;
+#define QM_TILE_CASE(TT, KK)                                                                                   \
+    case KK:                                                                                                   \
+        return launch_tile_sized<TT, KK>(amps, qubits, tp, terms, states, state_stride, partials, columns,    \
+                                         rows_per_state, mass_column, st);
+    if (precision == QM_FP32) {
+        switch (tp.k) {
+            QM_TILE_CASE(float, 9) QM_TILE_CASE(float, 10) QM_TILE_CASE(float, 11) QM_TILE_CASE(float, 12)
+        default: return cudaErrorInvalidValue;
+        }
+    }
+    switch (tp.k) {
+        QM_TILE_CASE(double, 9) QM_TILE_CASE(double, 10) QM_TILE_CASE(double, 11)
+    default: return cudaErrorInvalidValue;
+    }
+#undef QM_TILE_CASE
+}
+
+cudaError_t launch_finish_batched(const double* partials, int states, int rows, int columns, double* out,
+                                  cudaStream_t st) {
+    const int threads = 128;
+    dim3 grid((columns * 32 + threads - 1) / threads, states);
+    k_finish_batched<<<grid, threads, 0, st>>>(partials, rows, columns, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reset_batched(void* amps, int qubits, int precision, int states, cudaStream_t st) {
+    const uint64_t per = 1ull << qubits, total = per * (uint64_t)states;
+    const uint64_t blocks = std::min<uint64_t>((total + 255) / 256, 148ull * 32);
+    if (precision == QM_FP32) k_reset_batched<float><<<(unsigned)blocks, 256, 0, st>>>((float2*)amps, per, total);
+    else k_reset_batched<double><<<(unsigned)blocks, 256, 0, st>>>((double2*)amps, per, total);
+    return cudaGetLastError();
+}
+
+}  // namespace qm

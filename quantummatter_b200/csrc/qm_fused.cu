@@ -40,7 +40,16 @@ struct FusedLaunch {
     uint32_t reg_out_g[R];      // ... at store
     int32_t reg_in_l[R];        // local positions of the load layout
     int32_t pad[R];
+    // Batches: state b = blockIdx.y lives at s + b * state_stride; ops flagged kOpTable take
+    // their coefficients from table + b * table_stride + 8 * op.reserved.
+    const double* table;
+    uint64_t state_stride;
+    uint64_t table_stride;
     FusedOp ops[MAXOPS];
+};
+
+struct Coef {
+    double v[8];
 };
 
 // Shared-memory slot of local index j: the low row bits are XORed with a fold of the
@@ -70,10 +79,10 @@ struct Layout {
 };
 
 template <typename T, int M, bool REAL, bool CTRL>
-__device__ __forceinline__ void op_matrix(Cx<T> (&a)[NR], const FusedOp& op, const Layout& L) {
-    const T ar = (T)op.coef[0], br = (T)op.coef[2], cr = (T)op.coef[4], dr = (T)op.coef[6];
-    const T ai = REAL ? (T)0 : (T)op.coef[1], bi = REAL ? (T)0 : (T)op.coef[3];
-    const T ci = REAL ? (T)0 : (T)op.coef[5], di = REAL ? (T)0 : (T)op.coef[7];
+__device__ __forceinline__ void op_matrix(Cx<T> (&a)[NR], const FusedOp& op, const Coef& c, const Layout& L) {
+    const T ar = (T)c.v[0], br = (T)c.v[2], cr = (T)c.v[4], dr = (T)c.v[6];
+    const T ai = REAL ? (T)0 : (T)c.v[1], bi = REAL ? (T)0 : (T)c.v[3];
+    const T ci = REAL ? (T)0 : (T)c.v[5], di = REAL ? (T)0 : (T)c.v[7];
     const uint32_t cm = op.cmask_local;
 #pragma unroll
     for (int i = 0; i < NR; ++i) {
@@ -92,15 +101,15 @@ __device__ __forceinline__ void op_matrix(Cx<T> (&a)[NR], const FusedOp& op, con
 }
 
 template <typename T, bool REAL, bool CTRL>
-__device__ __forceinline__ void op_matrix_any(Cx<T> (&a)[NR], const FusedOp& op, const Layout& L) {
+__device__ __forceinline__ void op_matrix_any(Cx<T> (&a)[NR], const FusedOp& op, const Coef& c, const Layout& L) {
     switch (op.reg) {
-    case 0: op_matrix<T, 0, REAL, CTRL>(a, op, L); break;
-    case 1: op_matrix<T, 1, REAL, CTRL>(a, op, L); break;
+    case 0: op_matrix<T, 0, REAL, CTRL>(a, op, c, L); break;
+    case 1: op_matrix<T, 1, REAL, CTRL>(a, op, c, L); break;
 #if QM_REG_BITS > 3
-    case 2: op_matrix<T, 2, REAL, CTRL>(a, op, L); break;
-    default: op_matrix<T, 3, REAL, CTRL>(a, op, L); break;
+    case 2: op_matrix<T, 2, REAL, CTRL>(a, op, c, L); break;
+    default: op_matrix<T, 3, REAL, CTRL>(a, op, c, L); break;
 #else
-    default: op_matrix<T, 2, REAL, CTRL>(a, op, L); break;
+    default: op_matrix<T, 2, REAL, CTRL>(a, op, c, L); break;
 #endif
     }
 }
@@ -210,8 +219,9 @@ __device__ __forceinline__ void slots(const Layout& L, uint32_t (&s)[NR]) {
 }
 
 template <typename T>
-__device__ __forceinline__ void op_diag(Cx<T> (&a)[NR], const FusedOp& op, const Layout& L, uint32_t outer) {
-    const T ar = (T)op.coef[0], ai = (T)op.coef[1], dr = (T)op.coef[6], di = (T)op.coef[7];
+__device__ __forceinline__ void op_diag(Cx<T> (&a)[NR], const FusedOp& op, const Coef& c, const Layout& L,
+                                        uint32_t outer) {
+    const T ar = (T)c.v[0], ai = (T)c.v[1], dr = (T)c.v[6], di = (T)c.v[7];
     const bool a_one = op.flags & 1, d_one = op.flags & 2;
     const uint32_t cm = op.cmask_local;
     const int lt = op.local;
@@ -257,6 +267,8 @@ __global__ void __launch_bounds__(1 << (K - R), ((sizeof(T) == 8 && K == 12) || 
     V* tile = reinterpret_cast<V*>(smem_raw);
     const uint32_t t = threadIdx.x;
     const uint32_t outer = deposit(blockIdx.x, P.outer_mask);
+    s += (size_t)blockIdx.y * P.state_stride;
+    const double* table = P.table ? P.table + (size_t)blockIdx.y * P.table_stride : nullptr;
 
     Cx<T> a[NR];
     {
@@ -314,17 +326,28 @@ __global__ void __launch_bounds__(1 << (K - R), ((sizeof(T) == 8 && K == 12) || 
         }
         if ((outer & op.cmask_outer) != op.cmask_outer) continue;
         const bool ctrl = op.cmask_local != 0;
+        Coef c;
+        if (code == OP_MATRIX || code == OP_MATRIX_REAL || code == OP_DIAG) {
+            if (op.flags & kOpTable) {
+                const double* src = table + 8 * (size_t)op.reserved;
+#pragma unroll
+                for (int k = 0; k < 8; ++k) c.v[k] = __ldg(src + k);
+            } else {
+#pragma unroll
+                for (int k = 0; k < 8; ++k) c.v[k] = op.coef[k];
+            }
+        }
         switch (code) {
         case OP_MATRIX:
-            if (ctrl) op_matrix_any<T, false, true>(a, op, L);
-            else op_matrix_any<T, false, false>(a, op, L);
+            if (ctrl) op_matrix_any<T, false, true>(a, op, c, L);
+            else op_matrix_any<T, false, false>(a, op, c, L);
             break;
         case OP_MATRIX_REAL:
-            if (ctrl) op_matrix_any<T, true, true>(a, op, L);
-            else op_matrix_any<T, true, false>(a, op, L);
+            if (ctrl) op_matrix_any<T, true, true>(a, op, c, L);
+            else op_matrix_any<T, true, false>(a, op, c, L);
             break;
         case OP_EXCHANGE: op_exchange_any<T>(a, op, L); break;
-        case OP_DIAG: op_diag<T>(a, op, L, outer); break;
+        case OP_DIAG: op_diag<T>(a, op, c, L, outer); break;
         case OP_NEGATE: op_negate<T>(a, op, L); break;
         case OP_SWAP: op_swap_any<T>(a, op, L); break;
         default: break;
@@ -344,7 +367,8 @@ __global__ void __launch_bounds__(1 << (K - R), ((sizeof(T) == 8 && K == 12) || 
 }
 
 template <typename T, int K, int MAXOPS>
-cudaError_t launch_k(void* amps, int qubits, const FusedPass& p, const FusedOp* ops, cudaStream_t st) {
+cudaError_t launch_k(void* amps, int qubits, const FusedPass& p, const FusedOp* ops, const FusedBatch* batch,
+                     cudaStream_t st) {
     using V = typename Vec2<T>::type;
     FusedLaunch<MAXOPS> L;
     const uint32_t all = (1u << qubits) - 1u;
@@ -366,6 +390,10 @@ cudaError_t launch_k(void* amps, int qubits, const FusedPass& p, const FusedOp* 
     }
     L.op_count = p.op_count;
     for (int i = 0; i < p.op_count; ++i) L.ops[i] = ops[p.op_begin + i];
+    L.table = batch ? batch->table : nullptr;
+    L.state_stride = batch ? batch->state_stride : 0;
+    L.table_stride = batch ? batch->table_stride : 0;
+    const unsigned states = batch ? (unsigned)batch->states : 1u;
     const size_t smem = sizeof(V) << K;
     static bool configured = false;
     if (!configured) {
@@ -374,37 +402,39 @@ cudaError_t launch_k(void* amps, int qubits, const FusedPass& p, const FusedOp* 
         if (e != cudaSuccess) return e;
         configured = true;
     }
-    dim3 grid(1u << (qubits - K));
+    dim3 grid(1u << (qubits - K), states);
     k_fused<T, K, MAXOPS><<<grid, 1 << (K - R), smem, st>>>(reinterpret_cast<V*>(amps), L);
     return cudaGetLastError();
 }
 
 template <typename T, int K>
-cudaError_t launch_sized(void* amps, int qubits, const FusedPass& p, const FusedOp* ops, cudaStream_t st) {
-    if (p.op_count <= kSmallPassOps) return launch_k<T, K, kSmallPassOps>(amps, qubits, p, ops, st);
-    return launch_k<T, K, kMaxPassOps>(amps, qubits, p, ops, st);
+cudaError_t launch_sized(void* amps, int qubits, const FusedPass& p, const FusedOp* ops, const FusedBatch* batch,
+                         cudaStream_t st) {
+    if (p.op_count <= kSmallPassOps) return launch_k<T, K, kSmallPassOps>(amps, qubits, p, ops, batch, st);
+    return launch_k<T, K, kMaxPassOps>(amps, qubits, p, ops, batch, st);
 }
 
 }  // namespace
 
 cudaError_t launch_fused(void* amps, int qubits, int precision, const FusedPass& p, const FusedOp* ops,
-                         cudaStream_t st) {
+                         const FusedBatch* batch, cudaStream_t st) {
     if (p.k > qubits || p.op_count > kMaxPassOps || p.op_count < 0) return cudaErrorInvalidValue;
+    if (batch && (batch->states < 1 || batch->states > 65535)) return cudaErrorInvalidValue;
     if (precision == QM_FP32) {
         switch (p.k) {
-        case 9: return launch_sized<float, 9>(amps, qubits, p, ops, st);
-        case 10: return launch_sized<float, 10>(amps, qubits, p, ops, st);
-        case 11: return launch_sized<float, 11>(amps, qubits, p, ops, st);
-        case 12: return launch_sized<float, 12>(amps, qubits, p, ops, st);
-        case 13: return launch_sized<float, 13>(amps, qubits, p, ops, st);
+        case 9: return launch_sized<float, 9>(amps, qubits, p, ops, batch, st);
+        case 10: return launch_sized<float, 10>(amps, qubits, p, ops, batch, st);
+        case 11: return launch_sized<float, 11>(amps, qubits, p, ops, batch, st);
+        case 12: return launch_sized<float, 12>(amps, qubits, p, ops, batch, st);
+        case 13: return launch_sized<float, 13>(amps, qubits, p, ops, batch, st);
         default: return cudaErrorInvalidValue;
         }
     }
     switch (p.k) {
-    case 9: return launch_sized<double, 9>(amps, qubits, p, ops, st);
-    case 10: return launch_sized<double, 10>(amps, qubits, p, ops, st);
-    case 11: return launch_sized<double, 11>(amps, qubits, p, ops, st);
-    case 12: return launch_sized<double, 12>(amps, qubits, p, ops, st);
+    case 9: return launch_sized<double, 9>(amps, qubits, p, ops, batch, st);
+    case 10: return launch_sized<double, 10>(amps, qubits, p, ops, batch, st);
+    case 11: return launch_sized<double, 11>(amps, qubits, p, ops, batch, st);
+    case 12: return launch_sized<double, 12>(amps, qubits, p, ops, batch, st);
     default: return cudaErrorInvalidValue;
     }
 }

@@ -57,6 +57,8 @@ constexpr int kMaxPassOps = 352;    // ops per pass: 352 * 88 B + header <= 32 K
 constexpr int kSmallPassOps = 48;   // launch variant for short programs (smaller parameter copy)
 constexpr int kMaxPassGates = 170;  // gates absorbed per pass (stage changes add at most gates + 2)
 
+constexpr uint16_t kOpTable = 4;    // FusedOp::flags: coefficients come from the batch's table
+
 enum OpCode : uint8_t {
     OP_STAGE = 0,       // new register layout: reg_pos[0..R) local bit positions
     OP_MATRIX = 1,      // complex 2x2 on register bit `reg`
@@ -77,7 +79,7 @@ struct FusedOp {            // 88 bytes
     uint16_t flags;         // bit0: a == 1, bit1: d == 1 (diagonal)
     uint32_t cmask_outer;   // controls outside the block, as global-index bits
     uint32_t target_outer;  // outer target bit of a diagonal (global), 0 when local
-    uint32_t reserved;
+    uint32_t reserved;      // kOpTable: coefficient slot in the batch table
     double coef[8];         // a, b, c, d as (re, im)
 };
 
@@ -103,14 +105,24 @@ struct Plan {
 };
 
 // Builds the fused schedule (qm_planner.cpp).  Returns false with a message on error.
+// slots (optional, one per gate): batch-table coefficient slot of each gate, -1 for gates
+// whose coefficients are the same for every state of a batch.
 bool plan_fused(const std::vector<qm_gate>& gates, int qubits, int precision, int width, Plan& plan,
-                std::string& error);
+                std::string& error, const std::vector<int32_t>* slots = nullptr);
 int default_block_qubits(int qubits, int precision);
 
 // ---------------------------------------------------------------- launchers (qm_kernels.cu)
 cudaError_t launch_gate(void* amps, int qubits, int precision, const DevGate& g, cudaStream_t s);
+// A batch of equally sized states with one shared plan: state b at amps + b * state_stride
+// (elements); ops flagged kOpTable read 8 coefficients at table + b * table_stride + 8 * op.reserved.
+struct FusedBatch {
+    int32_t states;
+    uint64_t state_stride;
+    const double* table;
+    uint64_t table_stride;
+};
 cudaError_t launch_fused(void* amps, int qubits, int precision, const FusedPass& p, const FusedOp* ops,
-                         cudaStream_t s);
+                         const FusedBatch* batch, cudaStream_t s);
 cudaError_t launch_reset(void* amps, int qubits, int precision, cudaStream_t s);
 cudaError_t launch_convert_from_f64(void* dst_f32, const double* src_f64, int64_t n, cudaStream_t s);
 cudaError_t launch_convert_to_f64(double* dst_f64, const void* src_f32, int64_t n, cudaStream_t s);
@@ -133,6 +145,38 @@ cudaError_t launch_search(const void* amps, int qubits, int precision, const dou
                           int blocks, int chunk, const double* targets, int shots, double margin,
                           int64_t* out, cudaStream_t s);
 cudaError_t launch_collapse(void* amps, int qubits, int precision, int64_t outcome, cudaStream_t s);
+
+// ---------------------------------------------------------------- tiled expectation (qm_expect.cu)
+constexpr int kTileMaxTerms = 256;
+struct TileTerm {
+    uint32_t flip_local;   // flip mask in the tile's local bits
+    uint32_t sign;         // Z-sign mask over global bits
+    int32_t phase;         // y_count & 3
+    int32_t column;        // output column (term index)
+};
+struct TilePass {
+    int32_t k;
+    int32_t q[kMaxBlockQubits];  // tile qubits, ascending (the lowest qubits first)
+    uint32_t block_mask;
+    int32_t term_begin, term_count;
+    int32_t with_mass;
+    int32_t row_offset;          // first partial row of the pass (rows = 2^(n-k))
+};
+struct TilePlan {
+    std::vector<TilePass> passes;
+    std::vector<TileTerm> terms;
+    int32_t rows_per_state = 0;
+    int32_t columns = 0;         // terms + 1 (the mass)
+    int32_t mass_column = 0;
+};
+int tile_block_qubits(int qubits, int precision);
+bool plan_tiles(int qubits, int precision, const qm_pauli_term* terms, int count, TilePlan& plan, std::string& error);
+cudaError_t launch_expect_tile(const void* amps, int qubits, int precision, const TilePass& pass, const TileTerm* terms,
+                               int states, uint64_t state_stride, double* partials, int columns, int rows_per_state,
+                               int mass_column, cudaStream_t s);
+cudaError_t launch_finish_batched(const double* partials, int states, int rows, int columns, double* out,
+                                  cudaStream_t s);
+cudaError_t launch_reset_batched(void* amps, int qubits, int precision, int states, cudaStream_t s);
 
 }  // namespace qm
 

@@ -26,6 +26,7 @@ namespace {
 
 struct GInfo {
     qm_gate g;
+    int32_t slot;    // batch-table coefficient slot, -1 for constant coefficients
     bool diag;
     uint32_t touch;  // every qubit the gate reads
     uint32_t xmask;  // qubits acted on non-diagonally
@@ -38,6 +39,7 @@ inline int popc(uint32_t x) { return __builtin_popcount(x); }
 GInfo classify(const qm_gate& g) {
     GInfo gi{};
     gi.g = g;
+    gi.slot = -1;
     uint32_t tb = 1u << g.target;
     uint32_t sb = g.kernel == QM_KERNEL_SWAP ? (1u << g.swap_control) : 0u;
     gi.touch = tb | sb | g.control_mask;
@@ -84,7 +86,7 @@ int default_block_qubits(int qubits, int precision) {
 }
 
 bool plan_fused(const std::vector<qm_gate>& gates, int qubits, int precision, int width, Plan& plan,
-                std::string& error) {
+                std::string& error, const std::vector<int32_t>* slots) {
     plan.qubits = qubits;
     plan.precision = precision;
     plan.passes.clear();
@@ -101,6 +103,10 @@ bool plan_fused(const std::vector<qm_gate>& gates, int qubits, int precision, in
     // Per-gate path: requested explicitly (width 1) or the state is too small for a block
     // of at least 9 qubits (32 threads of 16 registers).
     if (width == 1 || k < 9) {
+        if (slots) {
+            error = "batched plans need a fused block of at least 9 qubits";
+            return false;
+        }
         plan.width = 1;
         for (const qm_gate& g : gates) {
             if (g.kernel == QM_KERNEL_IDENTITY) continue;
@@ -120,14 +126,23 @@ bool plan_fused(const std::vector<qm_gate>& gates, int qubits, int precision, in
 
     std::vector<GInfo> remaining;
     remaining.reserve(gates.size());
-    for (const qm_gate& g : gates) {
+    for (size_t gi = 0; gi < gates.size(); ++gi) {
+        const qm_gate& g = gates[gi];
+        const int32_t slot = slots ? (*slots)[gi] : -1;
         if (g.kernel == QM_KERNEL_IDENTITY) continue;
-        if (g.kernel == QM_KERNEL_DIAGONAL && is_exact(g.a, 1.0, 0.0) && is_exact(g.d, 1.0, 0.0)) continue;
+        if (slot < 0 && g.kernel == QM_KERNEL_DIAGONAL && is_exact(g.a, 1.0, 0.0) && is_exact(g.d, 1.0, 0.0)) continue;
         if (g.kernel == QM_KERNEL_SWAP && (g.swap_control < 0 || g.swap_control == g.target)) {
             error = "swap operands must be distinct";
             return false;
         }
-        remaining.push_back(classify(g));
+        if (slot >= 0 && g.kernel != QM_KERNEL_MATRIX && g.kernel != QM_KERNEL_HADAMARD &&
+            g.kernel != QM_KERNEL_DIAGONAL) {
+            error = "only matrix and diagonal gates can take per-state coefficients";
+            return false;
+        }
+        GInfo info = classify(g);
+        info.slot = slot;
+        remaining.push_back(info);
     }
 
     // Low qubits always in the block: 8 complex128 or 16 complex64 = one 128-byte run.
@@ -294,7 +309,21 @@ bool plan_fused(const std::vector<qm_gate>& gates, int qubits, int precision, in
                 std::memcpy(&op.coef[2], g.b, 16);
                 std::memcpy(&op.coef[4], g.c, 16);
                 std::memcpy(&op.coef[6], g.d, 16);
-                if (gi.diag) {
+                if (gi.slot >= 0) {
+                    // per-state coefficients: generic op reading the batch table
+                    op.flags = kOpTable;
+                    op.reserved = (uint32_t)gi.slot;
+                    if (gi.diag) {
+                        int lt = local_of[g.target];
+                        op.code = OP_DIAG;
+                        op.local = (int8_t)lt;
+                        op.target_outer = lt >= 0 ? 0u : (1u << g.target);
+                    } else {
+                        bool real = g.a[1] == 0 && g.b[1] == 0 && g.c[1] == 0 && g.d[1] == 0;
+                        op.code = real ? OP_MATRIX_REAL : OP_MATRIX;
+                        op.reg = (int8_t)reg_of_local[local_of[g.target]];
+                    }
+                } else if (gi.diag) {
                     bool a1 = is_exact(g.a, 1.0, 0.0), d1 = is_exact(g.d, 1.0, 0.0);
                     int lt = local_of[g.target];
                     if (a1 && is_exact(g.d, -1.0, 0.0)) {

@@ -61,3 +61,62 @@ def brick_circuit(qubits: int, depth: int, seed: int = DEFAULT_SEED) -> QuantumC
 
 def gate_count(circuit: QuantumCircuit) -> int:
     return len(circuit.Operations)
+
+
+def hardware_efficient_ansatz(qubits: int, layers: int = 4):
+    """Layers of RY on every qubit, RZ on every qubit, then a CZ ladder (i, i+1); 2 * qubits
+    parameters per layer, so P = 8 * qubits for four layers."""
+    from .variational import ParameterizedCircuit
+    c = ParameterizedCircuit(qubits, 2 * qubits * layers)
+    p = 0
+    for _ in range(layers):
+        for q in range(qubits):
+            c.Ry(q, p)
+            p += 1
+        for q in range(qubits):
+            c.Rz(q, p)
+            p += 1
+        ladder = QuantumCircuit(qubits)
+        for q in range(qubits - 1):
+            ladder.CZ(q, q + 1)
+        c.Append(ladder)
+    return c
+
+
+def xxz_chain(qubits: int, seed: int = DEFAULT_SEED):
+    """Open 1D Heisenberg XXZ chain: sum_i J_i (X_i X_{i+1} + Y_i Y_{i+1} + Delta_i Z_i Z_{i+1}) + sum_i h_i Z_i
+    with J ~ U[0.5, 1.5], Delta ~ U[0, 2], h ~ N(0, 0.3): 4n - 3 Pauli terms."""
+    from .observables import PauliHamiltonian, PauliString, PauliTerm
+    rng = SplitMix64(seed ^ (qubits * 0x9E37))
+
+    def label(pairs: dict[int, str]) -> str:
+        return "".join(pairs.get(q, "I") for q in reversed(range(qubits)))
+
+    terms = []
+    for i in range(qubits - 1):
+        j, delta = rng.uniform(0.5, 1.5), rng.uniform(0.0, 2.0)
+        terms.append(PauliTerm(j, PauliString(label({i: "X", i + 1: "X"}))))
+        terms.append(PauliTerm(j, PauliString(label({i: "Y", i + 1: "Y"}))))
+        terms.append(PauliTerm(j * delta, PauliString(label({i: "Z", i + 1: "Z"}))))
+    for i in range(qubits):
+        terms.append(PauliTerm(rng.normal(0.0, 0.3), PauliString(label({i: "Z"}))))
+    return PauliHamiltonian(qubits, terms)
+
+
+def tfim_chain(qubits: int, seed: int = DEFAULT_SEED):
+    """Transverse-field Ising chain H = -sum J Z_i Z_{i+1} - sum h X_i with J, h ~ U[0.5, 1.5]."""
+    from .observables import PauliHamiltonian, PauliString, PauliTerm
+    rng = SplitMix64(seed ^ (qubits * 0x51ED))
+
+    def label(pairs: dict[int, str]) -> str:
+        return "".join(pairs.get(q, "I") for q in reversed(range(qubits)))
+
+    terms = [PauliTerm(-rng.uniform(0.5, 1.5), PauliString(label({i: "Z", i + 1: "Z"}))) for i in range(qubits - 1)]
+    terms += [PauliTerm(-rng.uniform(0.5, 1.5), PauliString(label({i: "X"}))) for i in range(qubits)]
+    return PauliHamiltonian(qubits, terms)
+
+
+def uniform_parameters(count: int, vectors: int, lo: float, hi: float, seed: int = DEFAULT_SEED):
+    import numpy as np
+    rng = SplitMix64(seed)
+    return np.array([[rng.uniform(lo, hi) for _ in range(count)] for _ in range(vectors)], dtype=np.float64)

@@ -1,0 +1,174 @@
+"""Variational layer: binding semantics and the VQE solver's host logic (CPU), and the batched
+B200 energy/gradient evaluator against the oracle-composed reference evaluator (GPU)."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+import ref_variational as ref
+from quantummatter_b200.circuit import GateKind, QuantumCircuit
+from quantummatter_b200.errors import ArgumentError, ArgumentOutOfRangeError
+from quantummatter_b200.observables import PauliHamiltonian, PauliString, PauliTerm
+from quantummatter_b200.variational import (ParameterizedCircuit, VariationalEnergyResult, VqeOptions, VqeSolver,
+                                            VqeTerminationReason)
+from quantummatter_b200.workloads import hardware_efficient_ansatz, uniform_parameters, xxz_chain
+
+
+def Z(coefficient: float = 1.0, qubits: int = 1) -> PauliHamiltonian:
+    return PauliHamiltonian(qubits, [PauliTerm(coefficient, PauliString("I" * (qubits - 1) + "Z"))])
+
+
+# ---------------------------------------------------------------- CPU: template semantics
+
+def test_bind_appends_the_shift_after_one_occurrence():
+    """ParameterizedCircuit.cs:68-96: the shift is a separate same-axis gate, never added to the angle."""
+    c = ParameterizedCircuit(2, 2).Ry(0, 0).Append(QuantumCircuit(2).CNot(0, 1)).Rz(1, 1).Ry(1, 0)
+    b = c.BindWithRotationShift([1e100, 0.2], 2, math.pi / 2)
+    kinds = [(op.Kind, op.Target, op.Angle) for op in b.Operations]
+    assert kinds == [(GateKind.Ry, 0, 1e100), (GateKind.CNot, 1, 0.0), (GateKind.Rz, 1, 0.2),
+                     (GateKind.Ry, 1, 1e100), (GateKind.Ry, 1, math.pi / 2)]
+    assert c.RotationParameterIndices == (0, 1, 0) and c.OperationCount == 4
+    with pytest.raises(ArgumentError):
+        c.Bind([0.1])
+    with pytest.raises(ArgumentOutOfRangeError):
+        c.Bind([0.1, float("nan")])
+    with pytest.raises(ArgumentOutOfRangeError):
+        c.BindWithRotationShift([0.1, 0.2], 3, 1.0)
+
+
+class FakeEvaluator:
+    """Energy E(theta) = sum (theta_i - 1)^2 with exact gradients; counts calls."""
+
+    def __init__(self):
+        self.energies = 0
+        self.gradients = 0
+
+    def Evaluate(self, circuit, hamiltonian, params):
+        self.energies += 1
+        return float(sum((p - 1) ** 2 for p in params))
+
+    def EvaluateWithGradient(self, circuit, hamiltonian, params):
+        self.gradients += 1
+        return VariationalEnergyResult(float(sum((p - 1) ** 2 for p in params)), tuple(2 * (p - 1) for p in params))
+
+
+def test_vqe_solver_counts_and_termination_reasons():
+    """VqeSolverTests.cs:33-181: accounting of energies, gradients and circuits; stopping reasons."""
+    c = ParameterizedCircuit(1, 2).Ry(0, 0).Rz(0, 1)
+    h = Z()
+    fake = FakeEvaluator()
+    r = VqeSolver(fake, VqeOptions(GradientTolerance=1e-9, InitialStepSize=0.5)).Solve(c, h, [0.0, 3.0])
+    assert r.TerminationReason == VqeTerminationReason.GradientToleranceReached
+    assert np.allclose(r.Parameters, [1.0, 1.0]) and r.Energy == 0
+    assert r.GradientEvaluationCount == fake.gradients and r.EnergyEvaluationCount == fake.energies
+    assert r.CircuitEvaluationCount == r.EnergyEvaluationCount + 5 * r.GradientEvaluationCount
+    r = VqeSolver(FakeEvaluator(), VqeOptions(MaximumIterations=0)).Solve(c, h, [0.0, 0.0])
+    assert r.TerminationReason == VqeTerminationReason.IterationLimitReached and r.CircuitEvaluationCount == 1
+    r = VqeSolver(FakeEvaluator(), VqeOptions(MaximumCircuitEvaluations=5)).Solve(c, h, [0.0, 0.0])
+    assert r.TerminationReason == VqeTerminationReason.EvaluationLimitReached
+    with pytest.raises(ArgumentOutOfRangeError):
+        VqeOptions(BacktrackingFactor=1.0).Validate()
+
+
+# ---------------------------------------------------------------- GPU: batched evaluator
+
+@pytest.fixture(scope="module")
+def evaluator(gpu_context):
+    from quantummatter_b200.variational import B200VariationalEnergyEvaluator
+    return B200VariationalEnergyEvaluator(gpu_context)
+
+
+def near(a, b, tol=5e-12):
+    assert abs(a - b) <= tol, (a, b)
+
+
+@pytest.mark.gpu
+def test_reference_gradient_cases(evaluator):
+    """VariationalEnergyTests.cs:17-45: product rule for a shared parameter, a 1e100 angle, a 1e16
+    identity offset and a 1e308 coefficient."""
+    shared = ParameterizedCircuit(1, 2).Ry(0, 0).Ry(0, 0)
+    angle = 0.37
+    r = evaluator.EvaluateWithGradient(shared, Z(), [angle, 17])
+    near(math.cos(2 * angle), r.Energy)
+    near(-2 * math.sin(2 * angle), r.Gradient[0])
+    assert r.Gradient[1] == 0
+    single = ParameterizedCircuit(1, 1).Ry(0, 0)
+    huge = 1e100
+    r = evaluator.EvaluateWithGradient(single, Z(), [huge])
+    near(math.cos(huge), r.Energy)
+    near(-math.sin(huge), r.Gradient[0])
+    offset = PauliHamiltonian(1, [PauliTerm(1e16, PauliString("I")), PauliTerm(1, PauliString("Z"))])
+    near(-math.sin(angle), evaluator.EvaluateWithGradient(single, offset, [angle]).Gradient[0])
+    large = evaluator.EvaluateWithGradient(single, Z(1e308), [math.pi / 2])
+    assert abs(large.Gradient[0] / 1e308 + 1) <= 4e-12
+
+
+def random_template(qubits: int, params: int, seed: int) -> ParameterizedCircuit:
+    rng = np.random.default_rng(seed)
+    c = ParameterizedCircuit(qubits, params)
+    for _ in range(6 * qubits):
+        r = rng.random()
+        q = int(rng.integers(qubits))
+        if r < 0.5:
+            getattr(c, ("Rx", "Ry", "Rz")[int(rng.integers(3))])(q, int(rng.integers(params)))
+        else:
+            seg = QuantumCircuit(qubits)
+            other = (q + 1 + int(rng.integers(qubits - 1))) % qubits if qubits > 1 else q
+            if qubits > 1 and r < 0.75:
+                seg.CNot(q, other)
+            elif qubits > 1 and r < 0.85:
+                seg.CZ(q, other)
+            else:
+                seg.H(q).S(q)
+            c.Append(seg)
+    return c
+
+
+def random_hamiltonian(qubits: int, seed: int) -> PauliHamiltonian:
+    rng = np.random.default_rng(seed)
+    terms = [PauliTerm(float(rng.normal()), PauliString("".join(rng.choice(list("IXYZ"), size=qubits))))
+             for _ in range(2 * qubits + 3)]
+    return PauliHamiltonian(qubits, terms)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("qubits", [2, 5, 10, 12])
+def test_energy_and_gradient_match_the_oracle_evaluator(evaluator, qubits):
+    c = random_template(qubits, 4, seed=qubits)
+    h = random_hamiltonian(qubits, seed=100 + qubits)
+    params = uniform_parameters(4, 2, -math.pi, math.pi, seed=qubits)
+    batch = evaluator.EvaluateBatch(c, h, params, withGradient=True)
+    for v in range(2):
+        e, g = ref.energy_and_gradient(c, h, params[v])
+        scale = max(1.0, sum(abs(t.Coefficient) for t in h.Terms))
+        near(batch.Energies[v], e, 5e-12 * scale)
+        assert np.max(np.abs(batch.Gradients[v] - g)) <= 5e-12 * scale
+    assert batch.Circuits == 2 * (1 + 2 * len(c.RotationParameterIndices))
+
+
+@pytest.mark.gpu
+def test_batched_vectors_equal_single_evaluations_bit_for_bit(evaluator):
+    c = hardware_efficient_ansatz(10, 2)
+    h = xxz_chain(10)
+    params = uniform_parameters(c.ParameterCount, 5, -math.pi, math.pi, seed=3)
+    batch = evaluator.EvaluateBatch(c, h, params, withGradient=True)
+    for v in (0, 3):
+        one = evaluator.EvaluateBatch(c, h, params[v], withGradient=True)
+        assert one.Energies[0] == batch.Energies[v]
+        assert np.array_equal(one.Gradients[0], batch.Gradients[v])
+
+
+@pytest.mark.gpu
+def test_fp32_energies_within_1e6_of_the_fp64_oracle(gpu_context):
+    from quantummatter_b200.backend import FP32
+    from quantummatter_b200.variational import B200VariationalEnergyEvaluator
+    n = 16
+    c = hardware_efficient_ansatz(n, 4)
+    h = xxz_chain(n)
+    params = uniform_parameters(c.ParameterCount, 4, -math.pi, math.pi, seed=16)
+    fp32 = B200VariationalEnergyEvaluator(gpu_context, FP32).EvaluateBatch(c, h, params, withGradient=False)
+    for v in range(4):
+        want = ref.energy(c, h, params[v])
+        assert abs(fp32.Energies[v] - want) <= 1e-6, (fp32.Energies[v], want)
