@@ -219,17 +219,55 @@ int32_t validate_gates(const qm_gate* gates, int32_t count, int32_t qubits) {
 
 // ---------------------------------------------------------------- plan execution
 
+}  // namespace
+
+namespace qm {
+
+int32_t plan_upload(Plan& plan, cudaStream_t stream, void** buffer, size_t* buffer_bytes) {
+    if (plan.ops.empty() || plan.d_ops) return QM_OK;
+    const size_t bytes = plan.ops.size() * sizeof(FusedOp);
+    if (buffer) {
+        if (*buffer_bytes < bytes) {
+            if (*buffer) {
+                cudaStreamSynchronize(stream);
+                cudaFree(*buffer);
+            }
+            *buffer = nullptr;
+            *buffer_bytes = 0;
+            QM_CUDA(cudaMalloc(buffer, bytes * 2));
+            *buffer_bytes = bytes * 2;
+        }
+        plan.d_ops = static_cast<FusedOp*>(*buffer);
+        plan.borrowed = true;
+    } else {
+        QM_CUDA(cudaMalloc(&plan.d_ops, bytes));
+    }
+    QM_CUDA(cudaMemcpyAsync(plan.d_ops, plan.ops.data(), bytes, cudaMemcpyHostToDevice, stream));
+    return QM_OK;
+}
+
+void plan_release(Plan& plan) {
+    if (plan.d_ops && !plan.borrowed) cudaFree(plan.d_ops);  // cudaFree waits for work using the buffer
+    plan.d_ops = nullptr;
+    plan.borrowed = false;
+}
+
+}  // namespace qm
+
+namespace {
+
+// transient plans (one-shot executions) borrow the context's program buffer
 int32_t build_plan(qm_context* ctx, int32_t qubits, int32_t precision, const qm_gate* gates, int32_t count,
-                   int32_t width, Plan& plan) {
+                   int32_t width, Plan& plan, bool transient = false) {
     std::vector<qm_gate> list(gates, gates + count);
     std::string err;
     if (width == 0) width = ctx->fusion_width;
     if (!plan_fused(list, qubits, precision, width, plan, err)) return fail(QM_E_ARG, "planner: " + err);
-    return QM_OK;
+    if (transient) return plan_upload(plan, ctx->stream, &ctx->program, &ctx->program_bytes);
+    return plan_upload(plan, ctx->stream);
 }
 
-// Plans hold host memory only (each pass's program travels as a kernel parameter).
-void free_plan(Plan& plan) { plan.ops.clear(); }
+void free_plan(Plan& plan) { plan_release(plan); }
 
 // Launches the plan on `amps`.  With a cancel flag the stream is synchronised every 32
 // launches and the flag polled, as the reference bounds queued work
@@ -251,7 +289,7 @@ int32_t run_plan(qm_context* ctx, const Plan& plan, void* amps, const volatile i
         }
     } else {
         for (const FusedPass& p : plan.passes) {
-            QM_CUDA(launch_fused(amps, plan.qubits, plan.precision, p, plan.ops.data(), nullptr, ctx->stream));
+            QM_CUDA(launch_fused(amps, plan.qubits, plan.precision, p, plan.d_ops, nullptr, ctx->stream));
             int32_t rc = chunk_boundary();
             if (rc) return rc;
         }
@@ -364,6 +402,7 @@ extern "C" int32_t qm_context_destroy(qm_context* ctx) {
         if (ctx->scratch) cudaFree(ctx->scratch);
         if (ctx->host_scratch) cudaFreeHost(ctx->host_scratch);
         if (ctx->staging) cudaFree(ctx->staging);
+        if (ctx->program) cudaFree(ctx->program);
         if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
         if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
         if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -447,7 +486,7 @@ extern "C" int32_t qm_execute_host(qm_context* ctx, int32_t qubits, const qm_ope
     std::vector<qm_gate> gates((size_t)count);
     for (int32_t i = 0; i < count; ++i) prepare_one(ops[i], gates[(size_t)i]);
     Plan plan;
-    rc = build_plan(ctx, qubits, QM_FP64, gates.data(), count, 0, plan);
+    rc = build_plan(ctx, qubits, QM_FP64, gates.data(), count, 0, plan, true);
     if (rc) { free_plan(plan); return rc; }
     void* dev = nullptr;
     rc = device_buffer(ctx, (size_t)bytes, &dev);
@@ -826,7 +865,7 @@ extern "C" int32_t qm_execute(qm_state* st, const qm_gate* gates, int32_t count,
     std::lock_guard<std::recursive_mutex> lock(st->ctx->mu);
     QM_CUDA(cudaSetDevice(st->ctx->device));
     Plan plan;
-    rc = build_plan(st->ctx, st->qubits, st->precision, gates, count, width, plan);
+    rc = build_plan(st->ctx, st->qubits, st->precision, gates, count, width, plan, true);
     if (rc == QM_OK) rc = execute_plan(st, plan, profile);
     cudaStreamSynchronize(st->ctx->stream);
     free_plan(plan);

@@ -110,6 +110,9 @@ bool plan_tiles(int qubits, int precision, const qm_pauli_term* terms, int count
                 plan.terms.push_back(TileTerm{fl, term.sign_mask, term.y_count & 3, mine[at]});
             }
             p.term_count = (int32_t)plan.terms.size() - p.term_begin;
+            // terms sharing a flip mask sit together: the kernel evaluates them as a group
+            std::stable_sort(plan.terms.begin() + p.term_begin, plan.terms.end(),
+                             [](const TileTerm& x, const TileTerm& y) { return x.flip_local < y.flip_local; });
             plan.passes.push_back(p);
             row_offset += rows;
         } while (at < mine.size());
@@ -146,7 +149,7 @@ int32_t enqueue_plan(qm_batch* b, const Plan& plan, int states, const double* d_
                      cudaStream_t st) {
     FusedBatch fb{states, (uint64_t)1 << b->qubits, d_table, table_stride};
     for (const FusedPass& p : plan.passes)
-        QM_CUDA(launch_fused(b->amps, b->qubits, b->precision, p, plan.ops.data(), &fb, st));
+        QM_CUDA(launch_fused(b->amps, b->qubits, b->precision, p, plan.d_ops, &fb, st));
     return QM_OK;
 }
 
@@ -295,6 +298,12 @@ extern "C" int32_t qm_batch_execute(qm_batch* b, int32_t states, const qm_gate* 
     std::string err;
     if (width == 0) width = ctx->fusion_width;
     if (!plan_fused(list, b->qubits, b->precision, width, plan, err, &sl)) return fail(QM_E_ARG, "planner: " + err);
+    struct Release {
+        Plan& p;
+        ~Release() { plan_release(p); }
+    } release{plan};
+    rc = plan_upload(plan, ctx->stream);
+    if (rc) return rc;
     const size_t tbytes = sizeof(double) * (size_t)states * slot_count * 8;
     if (tbytes) {
         rc = grow(b->table, b->table_bytes, tbytes);
@@ -443,6 +452,14 @@ extern "C" int32_t qm_vqe_evaluate(qm_context* ctx, int32_t qubits, int32_t prec
     Plan plan;
     std::string err;
     if (!plan_fused(gates, qubits, precision, ctx->fusion_width, plan, err, &slots)) return fail(QM_E_ARG, "planner: " + err);
+    struct Release {
+        Plan& p;
+        ~Release() { plan_release(p); }
+    } release{plan};
+    {
+        int32_t urc = plan_upload(plan, ctx->stream);
+        if (urc) return urc;
+    }
     TilePlan tp;
     if (!plan_tiles(qubits, precision, terms, term_count, tp, err)) return fail(QM_E_ARG, err);
 

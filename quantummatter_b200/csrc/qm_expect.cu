@@ -44,7 +44,7 @@ __device__ __forceinline__ double warp_sum(double v) {
 }
 
 template <typename T, int K, int MAXT>
-__global__ void __launch_bounds__(1 << (K - R))
+__global__ void __launch_bounds__(1 << (K - R), 512 / (1 << (K - R)))
     k_expect_tile(const typename Vec2<T>::type* __restrict__ s, const __grid_constant__ TileLaunch<MAXT> P) {
     using V = typename Vec2<T>::type;
     constexpr int NT = 1 << (K - R);
@@ -58,7 +58,8 @@ __global__ void __launch_bounds__(1 << (K - R))
     const uint32_t outer = deposit(blockIdx.x, P.outer_mask);
     const uint32_t g0 = outer | deposit(t, P.thread_mask);
 
-    Cx<T> a[NR];
+    // stage the block; each thread later re-reads its own amplitudes from shared memory
+    // (keeping them in registers would cap occupancy at one CTA per SM)
     uint32_t g[NR];
 #pragma unroll
     for (int i = 0; i < NR; ++i) {
@@ -67,46 +68,67 @@ __global__ void __launch_bounds__(1 << (K - R))
         for (int m = 0; m < R; ++m)
             if ((i >> m) & 1) gi |= P.reg_g[m];
         g[i] = gi;
-        a[i] = load_amp<T>(s, gi);
-        V v;
-        v.x = a[i].re;
-        v.y = a[i].im;
-        tile[t | ((uint32_t)i << (K - R))] = v;
+        tile[t | ((uint32_t)i << (K - R))] = s[gi];
     }
     __syncthreads();
 
-    for (int k = 0; k < P.terms; ++k) {
-        const TileTerm term = P.t[k];
-        double acc = 0.0;
+    // Terms arrive sorted by flip mask; up to kGroup consecutive terms with the same mask share
+    // one partner load and one overlap per amplitude.
+    constexpr int kGroup = 4;
+    for (int k = 0; k < P.terms;) {
+        const uint32_t flip = P.t[k].flip_local;
+        int cnt = 1;
+        while (cnt < kGroup && k + cnt < P.terms && P.t[k + cnt].flip_local == flip) ++cnt;
+        uint32_t sign[kGroup];
+        int phase[kGroup];
+#pragma unroll
+        for (int u = 0; u < kGroup; ++u) {
+            sign[u] = u < cnt ? P.t[k + u].sign : 0u;
+            phase[u] = u < cnt ? P.t[k + u].phase : 0;
+        }
+        double acc[kGroup] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
         for (int i = 0; i < NR; ++i) {
-            const double ar = a[i].re, ai = a[i].im;
+            const V own = tile[t | ((uint32_t)i << (K - R))];
+            const double ar = own.x, ai = own.y;
             double ore, oim;
-            if (term.flip_local == 0) {
+            if (flip == 0) {
                 ore = ar * ar + ai * ai;
                 oim = 0.0;
             } else {
-                const V b = tile[(t | ((uint32_t)i << (K - R))) ^ term.flip_local];
+                const V b = tile[(t | ((uint32_t)i << (K - R))) ^ flip];
                 const double br = b.x, bi = b.y;
                 ore = br * ar + bi * ai;
                 oim = br * ai - bi * ar;
             }
-            double c;
-            switch (term.phase) {
-            case 0: c = ore; break;
-            case 1: c = -oim; break;
-            case 2: c = -ore; break;
-            default: c = oim; break;
+#pragma unroll
+            for (int u = 0; u < kGroup; ++u) {
+                if (u >= cnt) break;
+                double c;
+                switch (phase[u]) {
+                case 0: c = ore; break;
+                case 1: c = -oim; break;
+                case 2: c = -ore; break;
+                default: c = oim; break;
+                }
+                acc[u] += (__popc(g[i] & sign[u]) & 1) ? -c : c;
             }
-            acc += (__popc(g[i] & term.sign) & 1) ? -c : c;
         }
-        acc = warp_sum(acc);
-        if (lane == 0) red[warp * (P.terms + 1) + k] = acc;
+#pragma unroll
+        for (int u = 0; u < kGroup; ++u) {
+            if (u >= cnt) break;
+            const double v = warp_sum(acc[u]);
+            if (lane == 0) red[warp * (P.terms + 1) + k + u] = v;
+        }
+        k += cnt;
     }
     if (P.with_mass) {
         double acc = 0.0;
 #pragma unroll
-        for (int i = 0; i < NR; ++i) acc += (double)a[i].re * a[i].re + (double)a[i].im * a[i].im;
+        for (int i = 0; i < NR; ++i) {
+            const V own = tile[t | ((uint32_t)i << (K - R))];
+            acc += (double)own.x * own.x + (double)own.y * own.y;
+        }
         acc = warp_sum(acc);
         if (lane == 0) red[warp * (P.terms + 1) + P.terms] = acc;
     }

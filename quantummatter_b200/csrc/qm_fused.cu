@@ -13,12 +13,16 @@
 // The load and store use the first and last stage layouts directly whenever those keep
 // the lowest qubits on thread bits (coalesced), so most passes have no extra exchange.
 //
-// The op program is a __grid_constant__ kernel parameter: every op field is a uniform
-// load from the constant bank, so interpreting the program costs no memory traffic.
+// The kernel is persistent (grid = resident CTAs): each CTA stages the pass program into
+// shared memory once and then loops over (state, block) work items, so interpreting the
+// program costs uniform shared-memory loads only, and a batch state's coefficient row is
+// staged once per state change.
 //
 // The arithmetic per gate is the pair update of CudaStateVectorKernel.cs:63-75
 // (a*x + b*y, c*x + d*y) in the state's precision with fused multiply-adds.
 #include <cuda_runtime.h>
+
+#include <algorithm>
 
 #include "qm_device.cuh"
 #include "qm_internal.h"
@@ -30,7 +34,6 @@ namespace {
 constexpr int R = kRegBits;
 constexpr int NR = 1 << R;
 
-template <int MAXOPS>
 struct FusedLaunch {
     uint32_t outer_mask;        // qubits outside the block
     uint32_t thread_in;         // global mask of the block qubits that are thread bits at load
@@ -39,13 +42,16 @@ struct FusedLaunch {
     uint32_t reg_in_g[R];       // global bit of each register bit at load
     uint32_t reg_out_g[R];      // ... at store
     int32_t reg_in_l[R];        // local positions of the load layout
-    int32_t pad[R];
-    // Batches: state b = blockIdx.y lives at s + b * state_stride; ops flagged kOpTable take
-    // their coefficients from table + b * table_stride + 8 * op.reserved.
+    int32_t cta_shift;          // log2 of the CTAs (blocks) per state
+    int32_t states;
+    int32_t table_slots;        // coefficient slots per state (0 without a table)
+    int32_t pad;
+    const FusedOp* ops;         // the pass program in device memory
+    // Batches: state b lives at s + b * state_stride; ops flagged kOpTable take their
+    // coefficients from table + b * table_stride + 8 * op.reserved.
     const double* table;
     uint64_t state_stride;
     uint64_t table_stride;
-    FusedOp ops[MAXOPS];
 };
 
 struct Coef {
@@ -218,6 +224,24 @@ __device__ __forceinline__ void slots(const Layout& L, uint32_t (&s)[NR]) {
     }
 }
 
+// Diagonal whose target bit is a register bit M: the phase of each register is known at
+// compile time.
+template <typename T, int M>
+__device__ __forceinline__ void op_diag_reg(Cx<T> (&a)[NR], const FusedOp& op, const Coef& c, const Layout& L) {
+    const T ar = (T)c.v[0], ai = (T)c.v[1], dr = (T)c.v[6], di = (T)c.v[7];
+    const bool a_one = op.flags & 1, d_one = op.flags & 2;
+    const uint32_t cm = op.cmask_local;
+#pragma unroll
+    for (int i = 0; i < NR; ++i) {
+        if (cm != 0 && (L.local(i) & cm) != cm) continue;
+        if ((i >> M) & 1) {
+            if (!d_one) a[i] = cmul<T>(dr, di, a[i]);
+        } else if (!a_one) {
+            a[i] = cmul<T>(ar, ai, a[i]);
+        }
+    }
+}
+
 template <typename T>
 __device__ __forceinline__ void op_diag(Cx<T> (&a)[NR], const FusedOp& op, const Coef& c, const Layout& L,
                                         uint32_t outer) {
@@ -225,25 +249,35 @@ __device__ __forceinline__ void op_diag(Cx<T> (&a)[NR], const FusedOp& op, const
     const bool a_one = op.flags & 1, d_one = op.flags & 2;
     const uint32_t cm = op.cmask_local;
     const int lt = op.local;
+    bool bit;
     if (lt < 0) {
         // target outside the block: one phase for the whole CTA
-        const bool bit = (outer & op.target_outer) != 0;
-        if (bit ? d_one : a_one) return;
-        const T pr = bit ? dr : ar, pi = bit ? di : ai;
+        bit = (outer & op.target_outer) != 0;
+    } else {
 #pragma unroll
-        for (int i = 0; i < NR; ++i) {
-            if (cm != 0 && (L.local(i) & cm) != cm) continue;
-            a[i] = cmul<T>(pr, pi, a[i]);
+        for (int m = 0; m < R; ++m) {
+            if (L.pm[m] == (1u << lt)) {
+                switch (m) {
+                case 0: op_diag_reg<T, 0>(a, op, c, L); return;
+                case 1: op_diag_reg<T, 1>(a, op, c, L); return;
+#if QM_REG_BITS > 3
+                case 2: op_diag_reg<T, 2>(a, op, c, L); return;
+                default: op_diag_reg<T, 3>(a, op, c, L); return;
+#else
+                default: op_diag_reg<T, 2>(a, op, c, L); return;
+#endif
+                }
+            }
         }
-        return;
+        // target on a thread bit: one phase for all of this thread's registers
+        bit = ((L.base >> lt) & 1u) != 0;
     }
+    if (bit ? d_one : a_one) return;
+    const T pr = bit ? dr : ar, pi = bit ? di : ai;
 #pragma unroll
     for (int i = 0; i < NR; ++i) {
-        const uint32_t j = L.local(i);
-        if (cm != 0 && (j & cm) != cm) continue;
-        const bool bit = ((j >> lt) & 1u) != 0;
-        if (bit ? d_one : a_one) continue;
-        a[i] = cmul<T>(bit ? dr : ar, bit ? di : ai, a[i]);
+        if (cm != 0 && (L.local(i) & cm) != cm) continue;
+        a[i] = cmul<T>(pr, pi, a[i]);
     }
 }
 
@@ -258,125 +292,243 @@ __device__ __forceinline__ void op_negate(Cx<T> (&a)[NR], const FusedOp& op, con
     }
 }
 
-template <typename T, int K, int MAXOPS>
+template <typename T>
+__device__ __forceinline__ Cx<T> cmulc(Cx<T> x, Cx<T> y) {
+    return Cx<T>{x.re * y.re - x.im * y.im, x.re * y.im + x.im * y.re};
+}
+
+// A group of commuting diagonals applied as one phase per register.  Every member's factor
+// splits by where its qubits sit: outside the block or on a thread bit it is one value for
+// the whole thread (folded into u); on a register bit m it is a pair (zero-phase, one-phase)
+// multiplied into (az[m], on[m]); a negate on register bits flips the sign of the registers
+// whose index has those bits (a 16-bit pattern).  Then phase[i] = u * prod_m (i_m ? on : az)
+// is built as a product tree and applied once.
+template <typename T>
+__device__ __forceinline__ void op_diag_group(Cx<T> (&a)[NR], const FusedOp* members, int count, const double* table,
+                                              const Layout& L, uint32_t outer) {
+    Cx<T> u{(T)1, (T)0};
+    Cx<T> az[R], on[R];
+#pragma unroll
+    for (int m = 0; m < R; ++m) {
+        az[m] = Cx<T>{(T)1, (T)0};
+        on[m] = Cx<T>{(T)1, (T)0};
+    }
+    uint32_t negate = 0;  // bit i: register i changes sign
+    uint32_t regmask = 0;
+#pragma unroll
+    for (int m = 0; m < R; ++m) regmask |= L.pm[m];
+    for (int k = 0; k < count; ++k) {
+        const FusedOp& op = members[k];
+        if ((outer & op.cmask_outer) != op.cmask_outer) continue;
+        if (op.code == OP_NEGATE) {
+            const uint32_t cm = op.cmask_local;
+            if ((L.base & cm & ~regmask) != (cm & ~regmask)) continue;  // a thread-bit factor is zero
+            uint32_t rm = 0;                                             // register indices in the mask
+#pragma unroll
+            for (int m = 0; m < R; ++m)
+                if (cm & L.pm[m]) rm |= 1u << m;
+            uint32_t pattern = 0;
+#pragma unroll
+            for (int i = 0; i < NR; ++i)
+                if ((i & rm) == rm) pattern |= 1u << i;
+            negate ^= pattern;
+            continue;
+        }
+        // uncontrolled single-qubit diagonal
+        const double* src = (op.flags & kOpTable) ? table + 8 * (size_t)op.reserved : op.coef;
+        const Cx<T> pa{(T)src[0], (T)src[1]}, pd{(T)src[6], (T)src[7]};
+        const int lt = op.local;
+        if (lt >= 0 && (regmask & (1u << lt))) {
+#pragma unroll
+            for (int m = 0; m < R; ++m)
+                if (L.pm[m] == (1u << lt)) {
+                    az[m] = cmulc<T>(az[m], pa);
+                    on[m] = cmulc<T>(on[m], pd);
+                }
+            continue;
+        }
+        const bool bit = lt < 0 ? (outer & op.target_outer) != 0 : ((L.base >> lt) & 1u) != 0;
+        u = cmulc<T>(u, bit ? pd : pa);
+    }
+    // phase[i] = lo[i & low] * hi[i >> LB]: two small product tables instead of a full tree,
+    // to keep the live registers low
+    constexpr int LB = R / 2, HB = R - LB;
+    Cx<T> lo[1 << LB], hi[1 << HB];
+    lo[0] = Cx<T>{(T)1, (T)0};
+    hi[0] = u;
+#pragma unroll
+    for (int m = 0; m < LB; ++m)
+#pragma unroll
+        for (int i = (1 << m) - 1; i >= 0; --i) {
+            lo[i | (1 << m)] = cmulc<T>(lo[i], on[m]);
+            lo[i] = cmulc<T>(lo[i], az[m]);
+        }
+#pragma unroll
+    for (int m = 0; m < HB; ++m)
+#pragma unroll
+        for (int i = (1 << m) - 1; i >= 0; --i) {
+            hi[i | (1 << m)] = cmulc<T>(hi[i], on[LB + m]);
+            hi[i] = cmulc<T>(hi[i], az[LB + m]);
+        }
+#pragma unroll
+    for (int i = 0; i < NR; ++i) {
+        const Cx<T> p = cmulc<T>(lo[i & ((1 << LB) - 1)], hi[i >> LB]);
+        Cx<T> v = cmulc<T>(p, a[i]);
+        const bool neg = (negate >> i) & 1u;
+        a[i].re = neg ? -v.re : v.re;
+        a[i].im = neg ? -v.im : v.im;
+    }
+}
+
+
+// Shared memory: [block of 2^K amplitudes][pass program][coefficient row of the current state]
+template <typename T, int K>
+__host__ __device__ constexpr size_t tile_bytes() {
+    return sizeof(typename Vec2<T>::type) << K;
+}
+__host__ __device__ constexpr size_t program_bytes(int ops) { return ((size_t)ops * sizeof(FusedOp) + 15) & ~size_t(15); }
+
+// Persistent: each CTA loops over (state, block) work items, so the pass program is staged
+// into shared memory once per CTA and a state's coefficient row once per state change.
+template <typename T, int K>
 __global__ void __launch_bounds__(1 << (K - R), ((sizeof(T) == 8 && K == 12) || (sizeof(T) == 4 && K == 13)) ? 2 : 1)
-    // two CTAs per SM at the default widths: one exchanging with HBM while the other computes
-    k_fused(typename Vec2<T>::type* __restrict__ s, const __grid_constant__ FusedLaunch<MAXOPS> P) {
+    k_fused(typename Vec2<T>::type* __restrict__ s0, const __grid_constant__ FusedLaunch P) {
     using V = typename Vec2<T>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V* tile = reinterpret_cast<V*>(smem_raw);
+    FusedOp* prog = reinterpret_cast<FusedOp*>(smem_raw + tile_bytes<T, K>());
+    double* table = reinterpret_cast<double*>(smem_raw + tile_bytes<T, K>() + program_bytes(P.op_count));
     const uint32_t t = threadIdx.x;
-    const uint32_t outer = deposit(blockIdx.x, P.outer_mask);
-    s += (size_t)blockIdx.y * P.state_stride;
-    const double* table = P.table ? P.table + (size_t)blockIdx.y * P.table_stride : nullptr;
-
-    Cx<T> a[NR];
     {
-        const uint32_t g0 = outer | deposit(t, P.thread_in);
+        const uint2* src = reinterpret_cast<const uint2*>(P.ops);
+        uint2* dst = reinterpret_cast<uint2*>(prog);
+        const int words = P.op_count * (int)(sizeof(FusedOp) / sizeof(uint2));
+        for (int i = t; i < words; i += blockDim.x) dst[i] = __ldg(src + i);
+    }
+    const int64_t total = (int64_t)P.states << P.cta_shift;
+    const uint32_t cta_mask = (1u << P.cta_shift) - 1u;
+    int current = -1;
+    for (int64_t item = blockIdx.x; item < total; item += gridDim.x) {
+        const int b = (int)(item >> P.cta_shift);
+        const uint32_t cta = (uint32_t)item & cta_mask;
+        __syncthreads();  // program staged / previous block's exchanges finished
+        if (P.table_slots > 0 && b != current) {
+            const double* row = P.table + (size_t)b * P.table_stride;
+            for (int i = t; i < 8 * P.table_slots; i += blockDim.x) table[i] = __ldg(row + i);
+            __syncthreads();
+        }
+        current = b;
+        typename Vec2<T>::type* __restrict__ s = s0 + (size_t)b * P.state_stride;
+        const uint32_t outer = deposit(cta, P.outer_mask);
+
+        Cx<T> a[NR];
+        {
+            const uint32_t g0 = outer | deposit(t, P.thread_in);
+#pragma unroll
+            for (int i = 0; i < NR; ++i) {
+                uint32_t g = g0;
+#pragma unroll
+                for (int m = 0; m < R; ++m)
+                    if ((i >> m) & 1) g |= P.reg_in_g[m];
+                a[i] = load_amp<T>(s, g);
+            }
+        }
+
+        Layout L;
+        {
+            uint32_t regs = 0;
+#pragma unroll
+            for (int m = 0; m < R; ++m) {
+                L.pm[m] = 1u << P.reg_in_l[m];
+                regs |= L.pm[m];
+            }
+            L.base = deposit(t, ((1u << K) - 1u) & ~regs);
+        }
+
+        for (int o = 0; o < P.op_count; ++o) {
+            const FusedOp& op = prog[o];
+            const int code = op.code;
+            if (code == OP_STAGE) {
+                uint32_t sl[NR];
+                slots<T>(L, sl);
+                __syncthreads();
+#pragma unroll
+                for (int i = 0; i < NR; ++i) {
+                    V v;
+                    v.x = a[i].re;
+                    v.y = a[i].im;
+                    tile[sl[i]] = v;
+                }
+                uint32_t regs = 0;
+#pragma unroll
+                for (int m = 0; m < R; ++m) {
+                    L.pm[m] = 1u << op.reg_pos[m];
+                    regs |= L.pm[m];
+                }
+                L.base = deposit(t, ((1u << K) - 1u) & ~regs);
+                slots<T>(L, sl);
+                __syncthreads();
+#pragma unroll
+                for (int i = 0; i < NR; ++i) {
+                    V v = tile[sl[i]];
+                    a[i] = Cx<T>{v.x, v.y};
+                }
+                continue;
+            }
+            if (code == OP_DIAG_GROUP) {
+                const int count = (int)op.reserved;
+                op_diag_group<T>(a, prog + o + 1, count, table, L, outer);
+                o += count;
+                continue;
+            }
+            if ((outer & op.cmask_outer) != op.cmask_outer) continue;
+            const bool ctrl = op.cmask_local != 0;
+            Coef c;
+            if (code == OP_MATRIX || code == OP_MATRIX_REAL || code == OP_DIAG) {
+                const double* src = (op.flags & kOpTable) ? table + 8 * (size_t)op.reserved : op.coef;
+#pragma unroll
+                for (int k = 0; k < 8; ++k) c.v[k] = src[k];
+            }
+            switch (code) {
+            case OP_MATRIX:
+                if (ctrl) op_matrix_any<T, false, true>(a, op, c, L);
+                else op_matrix_any<T, false, false>(a, op, c, L);
+                break;
+            case OP_MATRIX_REAL:
+                if (ctrl) op_matrix_any<T, true, true>(a, op, c, L);
+                else op_matrix_any<T, true, false>(a, op, c, L);
+                break;
+            case OP_EXCHANGE: op_exchange_any<T>(a, op, L); break;
+            case OP_DIAG: op_diag<T>(a, op, c, L, outer); break;
+            case OP_NEGATE: op_negate<T>(a, op, L); break;
+            case OP_SWAP: op_swap_any<T>(a, op, L); break;
+            default: break;
+            }
+        }
+
+        // the planner ends every pass in the store layout
+        const uint32_t g0 = outer | deposit(t, P.thread_out);
 #pragma unroll
         for (int i = 0; i < NR; ++i) {
             uint32_t g = g0;
 #pragma unroll
             for (int m = 0; m < R; ++m)
-                if ((i >> m) & 1) g |= P.reg_in_g[m];
-            a[i] = load_amp<T>(s, g);
+                if ((i >> m) & 1) g |= P.reg_out_g[m];
+            store_amp<T>(s, g, a[i]);
         }
-    }
-
-    Layout L;
-    {
-        uint32_t regs = 0;
-#pragma unroll
-        for (int m = 0; m < R; ++m) {
-            L.pm[m] = 1u << P.reg_in_l[m];
-            regs |= L.pm[m];
-        }
-        L.base = deposit(t, ((1u << K) - 1u) & ~regs);
-    }
-
-    for (int o = 0; o < P.op_count; ++o) {
-        const FusedOp& op = P.ops[o];
-        const int code = op.code;
-        if (code == OP_STAGE) {
-            uint32_t sl[NR];
-            slots<T>(L, sl);
-            __syncthreads();
-#pragma unroll
-            for (int i = 0; i < NR; ++i) {
-                V v;
-                v.x = a[i].re;
-                v.y = a[i].im;
-                tile[sl[i]] = v;
-            }
-            uint32_t regs = 0;
-#pragma unroll
-            for (int m = 0; m < R; ++m) {
-                L.pm[m] = 1u << op.reg_pos[m];
-                regs |= L.pm[m];
-            }
-            L.base = deposit(t, ((1u << K) - 1u) & ~regs);
-            slots<T>(L, sl);
-            __syncthreads();
-#pragma unroll
-            for (int i = 0; i < NR; ++i) {
-                V v = tile[sl[i]];
-                a[i] = Cx<T>{v.x, v.y};
-            }
-            continue;
-        }
-        if ((outer & op.cmask_outer) != op.cmask_outer) continue;
-        const bool ctrl = op.cmask_local != 0;
-        Coef c;
-        if (code == OP_MATRIX || code == OP_MATRIX_REAL || code == OP_DIAG) {
-            if (op.flags & kOpTable) {
-                const double* src = table + 8 * (size_t)op.reserved;
-#pragma unroll
-                for (int k = 0; k < 8; ++k) c.v[k] = __ldg(src + k);
-            } else {
-#pragma unroll
-                for (int k = 0; k < 8; ++k) c.v[k] = op.coef[k];
-            }
-        }
-        switch (code) {
-        case OP_MATRIX:
-            if (ctrl) op_matrix_any<T, false, true>(a, op, c, L);
-            else op_matrix_any<T, false, false>(a, op, c, L);
-            break;
-        case OP_MATRIX_REAL:
-            if (ctrl) op_matrix_any<T, true, true>(a, op, c, L);
-            else op_matrix_any<T, true, false>(a, op, c, L);
-            break;
-        case OP_EXCHANGE: op_exchange_any<T>(a, op, L); break;
-        case OP_DIAG: op_diag<T>(a, op, c, L, outer); break;
-        case OP_NEGATE: op_negate<T>(a, op, L); break;
-        case OP_SWAP: op_swap_any<T>(a, op, L); break;
-        default: break;
-        }
-    }
-
-    // the planner ends every pass in the store layout
-    const uint32_t g0 = outer | deposit(t, P.thread_out);
-#pragma unroll
-    for (int i = 0; i < NR; ++i) {
-        uint32_t g = g0;
-#pragma unroll
-        for (int m = 0; m < R; ++m)
-            if ((i >> m) & 1) g |= P.reg_out_g[m];
-        store_amp<T>(s, g, a[i]);
     }
 }
 
-template <typename T, int K, int MAXOPS>
-cudaError_t launch_k(void* amps, int qubits, const FusedPass& p, const FusedOp* ops, const FusedBatch* batch,
+template <typename T, int K>
+cudaError_t launch_k(void* amps, int qubits, const FusedPass& p, const FusedOp* d_ops, const FusedBatch* batch,
                      cudaStream_t st) {
     using V = typename Vec2<T>::type;
-    FusedLaunch<MAXOPS> L;
+    FusedLaunch L;
     const uint32_t all = (1u << qubits) - 1u;
     L.outer_mask = all & ~p.block_mask;
     uint32_t reg_in_local = 0, reg_out_local = 0;
     for (int m = 0; m < R; ++m) {
         L.reg_in_l[m] = p.reg_in[m];
-        L.pad[m] = 0;
         L.reg_in_g[m] = 1u << p.q[p.reg_in[m]];
         L.reg_out_g[m] = 1u << p.q[p.reg_out[m]];
         reg_in_local |= 1u << p.reg_in[m];
@@ -389,52 +541,59 @@ cudaError_t launch_k(void* amps, int qubits, const FusedPass& p, const FusedOp* 
         if (!(reg_out_local & (1u << b))) L.thread_out |= 1u << p.q[b];
     }
     L.op_count = p.op_count;
-    for (int i = 0; i < p.op_count; ++i) L.ops[i] = ops[p.op_begin + i];
+    L.ops = d_ops + p.op_begin;
+    L.cta_shift = qubits - K;
+    L.states = batch ? batch->states : 1;
     L.table = batch ? batch->table : nullptr;
     L.state_stride = batch ? batch->state_stride : 0;
     L.table_stride = batch ? batch->table_stride : 0;
-    const unsigned states = batch ? (unsigned)batch->states : 1u;
-    const size_t smem = sizeof(V) << K;
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e =
-            cudaFuncSetAttribute(k_fused<T, K, MAXOPS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        configured = true;
+    L.table_slots = (batch && batch->table) ? (int32_t)(batch->table_stride / 8) : 0;
+    L.pad = 0;
+    const size_t smem = tile_bytes<T, K>() + program_bytes(p.op_count) + sizeof(double) * 8 * (size_t)L.table_slots;
+    static int optin = 0, sms = 0;
+    if (!optin) {
+        int dev = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+        if (e != cudaSuccess) {
+            optin = 0;
+            return e;
+        }
     }
-    dim3 grid(1u << (qubits - K), states);
-    k_fused<T, K, MAXOPS><<<grid, 1 << (K - R), smem, st>>>(reinterpret_cast<V*>(amps), L);
+    if (smem > (size_t)optin) return cudaErrorInvalidValue;  // program or coefficient row too large
+    int per_sm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fused<T, K>, 1 << (K - R), smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorInvalidConfiguration;
+    const int64_t items = (int64_t)L.states << L.cta_shift;
+    const int64_t grid = std::min<int64_t>(items, (int64_t)sms * per_sm);
+    k_fused<T, K><<<(unsigned)grid, 1 << (K - R), smem, st>>>(reinterpret_cast<V*>(amps), L);
     return cudaGetLastError();
-}
-
-template <typename T, int K>
-cudaError_t launch_sized(void* amps, int qubits, const FusedPass& p, const FusedOp* ops, const FusedBatch* batch,
-                         cudaStream_t st) {
-    if (p.op_count <= kSmallPassOps) return launch_k<T, K, kSmallPassOps>(amps, qubits, p, ops, batch, st);
-    return launch_k<T, K, kMaxPassOps>(amps, qubits, p, ops, batch, st);
 }
 
 }  // namespace
 
-cudaError_t launch_fused(void* amps, int qubits, int precision, const FusedPass& p, const FusedOp* ops,
+cudaError_t launch_fused(void* amps, int qubits, int precision, const FusedPass& p, const FusedOp* d_ops,
                          const FusedBatch* batch, cudaStream_t st) {
-    if (p.k > qubits || p.op_count > kMaxPassOps || p.op_count < 0) return cudaErrorInvalidValue;
+    if (p.k > qubits || p.op_count > kMaxPassOps || p.op_count < 0 || !d_ops) return cudaErrorInvalidValue;
     if (batch && (batch->states < 1 || batch->states > 65535)) return cudaErrorInvalidValue;
     if (precision == QM_FP32) {
         switch (p.k) {
-        case 9: return launch_sized<float, 9>(amps, qubits, p, ops, batch, st);
-        case 10: return launch_sized<float, 10>(amps, qubits, p, ops, batch, st);
-        case 11: return launch_sized<float, 11>(amps, qubits, p, ops, batch, st);
-        case 12: return launch_sized<float, 12>(amps, qubits, p, ops, batch, st);
-        case 13: return launch_sized<float, 13>(amps, qubits, p, ops, batch, st);
+        case 9: return launch_k<float, 9>(amps, qubits, p, d_ops, batch, st);
+        case 10: return launch_k<float, 10>(amps, qubits, p, d_ops, batch, st);
+        case 11: return launch_k<float, 11>(amps, qubits, p, d_ops, batch, st);
+        case 12: return launch_k<float, 12>(amps, qubits, p, d_ops, batch, st);
+        case 13: return launch_k<float, 13>(amps, qubits, p, d_ops, batch, st);
         default: return cudaErrorInvalidValue;
         }
     }
     switch (p.k) {
-    case 9: return launch_sized<double, 9>(amps, qubits, p, ops, batch, st);
-    case 10: return launch_sized<double, 10>(amps, qubits, p, ops, batch, st);
-    case 11: return launch_sized<double, 11>(amps, qubits, p, ops, batch, st);
-    case 12: return launch_sized<double, 12>(amps, qubits, p, ops, batch, st);
+    case 9: return launch_k<double, 9>(amps, qubits, p, d_ops, batch, st);
+    case 10: return launch_k<double, 10>(amps, qubits, p, d_ops, batch, st);
+    case 11: return launch_k<double, 11>(amps, qubits, p, d_ops, batch, st);
+    case 12: return launch_k<double, 12>(amps, qubits, p, d_ops, batch, st);
     default: return cudaErrorInvalidValue;
     }
 }

@@ -53,9 +53,8 @@ DevGate to_dev_gate(const qm_gate& g);
 #endif
 constexpr int kRegBits = QM_REG_BITS;
 constexpr int kMaxBlockQubits = 14;
-constexpr int kMaxPassOps = 352;    // ops per pass: 352 * 88 B + header <= 32 KB of parameters
-constexpr int kSmallPassOps = 48;   // launch variant for short programs (smaller parameter copy)
-constexpr int kMaxPassGates = 170;  // gates absorbed per pass (stage changes add at most gates + 2)
+constexpr int kMaxPassOps = 256;    // ops per pass: the program (88 B per op) is staged in shared memory
+constexpr int kMaxPassGates = 120;  // gates absorbed per pass (stage changes add at most gates + 2)
 
 constexpr uint16_t kOpTable = 4;    // FusedOp::flags: coefficients come from the batch's table
 
@@ -67,6 +66,8 @@ enum OpCode : uint8_t {
     OP_DIAG = 4,        // diagonal: a on bit-zero, d on bit-one of local bit `local` (or outer bit)
     OP_NEGATE = 5,      // amplitude *= -1 where all of (cmask_local, cmask_outer) bits are set: CZ, Z
     OP_SWAP = 6,        // exchange register bits `reg` and `reg2`
+    OP_DIAG_GROUP = 7,  // the next `reserved` ops are commuting diagonals (uncontrolled OP_DIAG,
+                        // OP_NEGATE on at most two bits) applied together as one phase per register
 };
 
 struct FusedOp {            // 88 bytes
@@ -100,9 +101,16 @@ struct Plan {
     std::vector<DevGate> gates;     // per-gate path
     std::vector<FusedPass> passes;  // fused path
     std::vector<FusedOp> ops;
+    FusedOp* d_ops = nullptr;       // device copy of ops (each pass's program is staged from it)
+    bool borrowed = false;          // d_ops belongs to a context buffer
     int64_t planned_bytes = 0;
     int32_t launches = 0;
 };
+// Copies the plan's program to the device (stream-ordered) / frees it.  With `buffer`, the
+// program goes into that growable device buffer instead of a new allocation (transient plans
+// of one-shot executions).
+int32_t plan_upload(Plan& plan, cudaStream_t stream, void** buffer = nullptr, size_t* buffer_bytes = nullptr);
+void plan_release(Plan& plan);
 
 // Builds the fused schedule (qm_planner.cpp).  Returns false with a message on error.
 // slots (optional, one per gate): batch-table coefficient slot of each gate, -1 for gates
@@ -198,9 +206,12 @@ struct qm_context {
     size_t scratch_bytes = 0;
     double* host_scratch = nullptr;   // pinned, for small downloads
     size_t host_scratch_bytes = 0;
-    // pinned staging for pageable host buffers (qm_execute_host)
+    // device buffer of the host-buffer entry points (qm_execute_host, qm_noise_apply_host)
     void* staging = nullptr;
     size_t staging_bytes = 0;
+    // device copy of the op program of one-shot executions (reused, grows as needed)
+    void* program = nullptr;
+    size_t program_bytes = 0;
 };
 
 struct qm_state {

@@ -295,6 +295,24 @@ bool plan_fused(const std::vector<qm_gate>& gates, int qubits, int precision, in
                 for (int b = 0; b < k; ++b)
                     if (layout & (1u << b)) reg_of_local[b] = m++;
             }
+            // Commuting diagonals (uncontrolled phases, CZ/Z negates) collect in a group that is
+            // emitted as one OP_DIAG_GROUP; a non-diagonal gate may run ahead of the group when
+            // its target is none of the group's qubits (they commute), otherwise the group is
+            // emitted first.
+            std::vector<FusedOp> group;
+            uint32_t group_qubits = 0;
+            auto flush = [&]() {
+                if (group.size() > 1) {
+                    FusedOp hdr{};
+                    hdr.code = OP_DIAG_GROUP;
+                    hdr.reg = hdr.reg2 = hdr.local = -1;
+                    hdr.reserved = (uint32_t)group.size();
+                    plan.ops.push_back(hdr);
+                }
+                for (const FusedOp& m : group) plan.ops.push_back(m);
+                group.clear();
+                group_qubits = 0;
+            };
             for (const GInfo& gi : stage_gates[si]) {
                 const qm_gate& g = gi.g;
                 FusedOp op{};
@@ -359,8 +377,18 @@ bool plan_fused(const std::vector<qm_gate>& gates, int qubits, int precision, in
                     error = "planner placed a swap outside the register layout";
                     return false;
                 }
+                const bool groupable =
+                    (op.code == OP_DIAG && op.cmask_local == 0 && op.cmask_outer == 0) ||
+                    (op.code == OP_NEGATE && popc(op.cmask_local) + popc(op.cmask_outer) <= 2);
+                if (groupable) {
+                    group.push_back(op);
+                    group_qubits |= gi.touch;
+                    continue;
+                }
+                if (!gi.diag && (gi.xmask & group_qubits)) flush();
                 plan.ops.push_back(op);
             }
+            flush();
         }
         if (layout & low_local) {
             emit_stage(canonical);

@@ -14,7 +14,7 @@ import numpy as np
 
 from quantummatter_b200 import _lib
 
-OP_STAGE, OP_MATRIX, OP_MATRIX_REAL, OP_EXCHANGE, OP_DIAG, OP_NEGATE, OP_SWAP = range(7)
+OP_STAGE, OP_MATRIX, OP_MATRIX_REAL, OP_EXCHANGE, OP_DIAG, OP_NEGATE, OP_SWAP, OP_DIAG_GROUP = range(8)
 
 
 def program(qubits: int, precision: int, gates, count: int, width: int):
@@ -52,11 +52,22 @@ def emulate(state: np.ndarray, qubits: int, passes, ops, reg_bits: int = 4) -> n
         blk = s[idx]
         layout = list(p.reg_in)
         assert all(b >= 3 for b in layout), "the load layout keeps the lowest qubits on thread bits"
+        pending_members = 0
         for op in ops[p.op_begin:p.op_begin + p.op_count]:
             if op.code == OP_STAGE:
                 layout = list(op.reg_pos)
                 assert len(set(layout)) == reg_bits and all(0 <= b < k for b in layout)
                 continue
+            if op.code == OP_DIAG_GROUP:
+                # the members follow; the kernel applies them together, the emulator one by one
+                assert op.reserved >= 2
+                pending_members = op.reserved
+                continue
+            if pending_members:
+                bits = bin(op.cmask_local).count("1") + bin(op.cmask_outer).count("1")
+                assert (op.code == OP_DIAG and op.cmask_local == 0 and op.cmask_outer == 0) or \
+                    (op.code == OP_NEGATE and bits <= 2), "a group holds only commuting phases and negates"
+                pending_members -= 1
             cta_ok = (outer & op.cmask_outer) == op.cmask_outer
             ctl = (local & op.cmask_local) == op.cmask_local
             a, b, c, d = (complex(op.coef[2 * i], op.coef[2 * i + 1]) for i in range(4))

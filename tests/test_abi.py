@@ -113,6 +113,45 @@ def test_planner_brick_circuit_pass_counts_and_bytes():
     assert np.max(np.abs(got - orc.execute(c, psi))) <= 1e-12
 
 
+def diagonal_heavy_circuit(qubits: int, gates: int, seed: int) -> QuantumCircuit:
+    """Mostly commuting diagonals (phases, CZ, Z) between a few rotations and CNOTs: exercises the
+    planner's diagonal groups, including controlled phases that stay outside the groups."""
+    rng = np.random.default_rng(seed)
+    c = QuantumCircuit(qubits)
+    for _ in range(gates):
+        q = int(rng.integers(qubits))
+        o = (q + 1 + int(rng.integers(qubits - 1))) % qubits
+        r = rng.random()
+        if r < 0.2:
+            c.Rz(q, float(rng.uniform(-3, 3)))
+        elif r < 0.3:
+            c.Phase(q, float(rng.uniform(-3, 3)))
+        elif r < 0.4:
+            (c.S, c.T, c.Z, c.Sdg)[int(rng.integers(4))](q)
+        elif r < 0.6:
+            c.CZ(q, o)
+        elif r < 0.67:
+            c.CPhase(q, o, float(rng.uniform(-3, 3)))
+        elif r < 0.85:
+            c.Ry(q, float(rng.uniform(-3, 3)))
+        elif r < 0.93:
+            c.H(q)
+        else:
+            c.CNot(q, o)
+    return c
+
+
+@pytest.mark.parametrize("width", [9, 11])
+def test_planner_groups_commuting_diagonals(width):
+    for seed in range(3):
+        c = diagonal_heavy_circuit(12, 250, seed)
+        gates, count = prepare(c)
+        passes, ops, _ = pe.program(12, 0, gates, count, width)
+        assert any(op.code == pe.OP_DIAG_GROUP for op in ops)
+        psi = random_state(12, seed)
+        assert np.max(np.abs(pe.emulate(psi, 12, passes, ops) - orc.execute(c, psi))) <= 1e-12
+
+
 def test_per_gate_width_counts_one_launch_per_gate():
     c = brick_circuit(10, 3, seed=1)
     gates, count = prepare(c)

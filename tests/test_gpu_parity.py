@@ -71,6 +71,21 @@ def test_random_circuits_fp64_match_the_oracle(gpu_context, width):
         assert np.max(np.abs(got - orc.execute(c, psi))) <= 3e-12
 
 
+@pytest.mark.parametrize("width", [9, 12])
+def test_diagonal_heavy_circuits_match_the_oracle(gpu_context, width):
+    """Groups of commuting phases and CZ/Z negates applied as one phase per register."""
+    from test_abi import diagonal_heavy_circuit
+    for seed, n in ((0, 12), (1, 14)):
+        c = diagonal_heavy_circuit(n, 400, seed)
+        psi = random_state(n, seed)
+        for precision, tol in ((FP64, 3e-12), (FP32, 5e-5)):
+            with DeviceState(gpu_context, n, precision) as st:
+                st.Upload(psi)
+                st.Evolve(c, fusion_width=width)
+                got = st.Download()
+            assert np.max(np.abs(got - orc.execute(c, psi))) <= tol, precision
+
+
 def test_brick_20_qubits_matches_the_oracle_within_1e12(gpu_context):
     """20 qubits, depth 20: 400 U3 + 190 CNOT from |0...0>, full 2^20-amplitude vector."""
     c = brick_circuit(20, 20)
