@@ -146,6 +146,13 @@ cudaError_t launch_expectation(const void* amps, int qubits, int precision, cons
                                int terms, double* scratch, int* blocks_out, cudaStream_t s);
 cudaError_t launch_finish_sums(const double* partials, int blocks, int columns, double* out,
                                cudaStream_t s);
+// One group of at most 8 terms sharing a flip mask into the [blocks][columns] partial table,
+// blocks = expectation_blocks(qubits) (at most 592).
+constexpr int kPauliGroupMax = 8;
+int expectation_blocks(int qubits);
+cudaError_t launch_pauli_group(const void* amps, int qubits, int precision, uint32_t flip, int terms,
+                               const uint32_t* sign, const int32_t* phase, const int32_t* column, int with_mass,
+                               int mass_column, int columns, double* partials, cudaStream_t s);
 // Sampling: per-block probability sums, then searches.
 cudaError_t launch_block_probs(const void* amps, int qubits, int precision, double* block_sums,
                                int64_t* block_last, int* blocks_out, int* chunk_out, cudaStream_t s);

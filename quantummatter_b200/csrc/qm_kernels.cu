@@ -533,6 +533,34 @@ cudaError_t launch_expectation(const void* amps, int qubits, int precision, cons
     return cudaSuccess;
 }
 
+int expectation_blocks(int qubits) { return reduce_blocks(1ull << qubits); }
+
+cudaError_t launch_pauli_group(const void* amps, int qubits, int precision, uint32_t flip, int terms,
+                               const uint32_t* sign, const int32_t* phase, const int32_t* column, int with_mass,
+                               int mass_column, int columns, double* partials, cudaStream_t st) {
+    if (terms < 0 || terms > kGroupMax) return cudaErrorInvalidValue;
+    const uint64_t n = 1ull << qubits;
+    GroupLaunch L{};
+    L.flip = flip;
+    L.low = flip ? __builtin_ctz(flip) : -1;
+    L.terms = terms;
+    L.with_mass = with_mass;
+    for (int t = 0; t < terms; ++t) {
+        L.sign[t] = sign[t];
+        L.phase[t] = phase[t] & 3;
+        L.column[t] = column[t];
+    }
+    L.columns = columns;
+    L.mass_column = mass_column;
+    const uint32_t items = L.low < 0 ? (uint32_t)n : (uint32_t)(n >> 1);
+    const int blocks = reduce_blocks(n);
+    if (precision == QM_FP32)
+        k_pauli_group<float><<<blocks, kThreads, 0, st>>>((const float2*)amps, items, L, partials);
+    else
+        k_pauli_group<double><<<blocks, kThreads, 0, st>>>((const double2*)amps, items, L, partials);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_finish_sums(const double* partials, int rows, int columns, double* out, cudaStream_t st) {
     int threads = 128;
     int blocks = (columns * 32 + threads - 1) / threads;
