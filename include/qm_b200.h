@@ -333,6 +333,30 @@ int32_t qm_vqe_evaluate(qm_context* context, int32_t qubits, int32_t precision, 
                         int32_t term_count, const double* parameters, int32_t vectors, int32_t with_gradient,
                         double* energies, double* gradients, qm_vqe_stats* stats);
 
+/* ---------------------------------------------------------------- allocation-free expectation */
+
+/* No counterpart in the reference: an additive entry point for hosts that cannot allocate
+ * device memory at the call (their pool allocator owns the device memory, or the device-wide
+ * synchronisation of cudaMalloc/cudaFree is not acceptable in their loop).
+ *
+ * Same results as qm_expectation_pauli on a caller-owned device state: per_term[t] =
+ * <psi|P_t|psi> / <psi|psi> (coefficients ignored), *mass = <psi|psi> (mass may be NULL),
+ * FP64 accumulation, QM_E_MASS as there.  `amplitudes` is the device address of 2^qubits
+ * interleaved (re, im) pairs, complex128 for QM_FP64 or complex64 for QM_FP32, on the current
+ * device; the kernels run on `stream` (NULL: the legacy default stream) and the call returns
+ * after that stream has finished them.
+ *
+ * It allocates nothing: its scratch (the reduction's per-block partial sums) is a fixed
+ * file-scope device array of about 304 KB per device, zeroed by the call itself.  The first
+ * call on each device looks that array's address up (cudaGetSymbolAddress); make that first
+ * call before any stream capture begins.  count > QM_NOALLOC_MAX_TERMS gives QM_E_RANGE.
+ * Calls whose work can overlap on one GPU (from several host threads, or on several streams)
+ * race on that device's scratch and give wrong sums: serialise them. */
+#define QM_NOALLOC_MAX_TERMS 64
+int32_t qm_expectation_pauli_noalloc(const void* amplitudes, int32_t qubits, int32_t precision,
+                                     const qm_pauli_term* terms, int32_t count, double* per_term,
+                                     double* mass, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

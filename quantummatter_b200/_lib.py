@@ -78,6 +78,8 @@ class VqeStats(C.Structure):
 
 NEXT_DOUBLE_FN = C.CFUNCTYPE(C.c_double, C.c_void_p)
 
+NOALLOC_MAX_TERMS = 64  # QM_NOALLOC_MAX_TERMS
+
 P = C.c_void_p
 I32 = C.c_int32
 I64 = C.c_int64
@@ -127,6 +129,7 @@ SIGNATURES = {
     "qm_batch_expectation": (I32, [P, I32, C.POINTER(PauliTermC), I32, DP, DP]),
     "qm_vqe_evaluate": (I32, [P, I32, I32, C.POINTER(TemplateOp), I32, I32, C.POINTER(PauliTermC), I32, DP, I32, I32,
                               DP, DP, C.POINTER(VqeStats)]),
+    "qm_expectation_pauli_noalloc": (I32, [P, I32, I32, C.POINTER(PauliTermC), I32, DP, DP, P]),
 }
 
 _lock = threading.Lock()

@@ -35,6 +35,8 @@ def test_library_exports_every_declared_entry_point():
     assert not missing, missing
     assert names == set(_lib.SIGNATURES), "the ctypes binding covers exactly the header"
     assert lib.qm_abi_version() == 1
+    limit = re.search(r"#define QM_NOALLOC_MAX_TERMS (\d+)", HEADER.read_text())
+    assert limit and int(limit.group(1)) == _lib.NOALLOC_MAX_TERMS
 
 
 def test_struct_layouts_match_the_header():
