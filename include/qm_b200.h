@@ -333,6 +333,66 @@ int32_t qm_vqe_evaluate(qm_context* context, int32_t qubits, int32_t precision, 
                         int32_t term_count, const double* parameters, int32_t vectors, int32_t with_gradient,
                         double* energies, double* gradients, qm_vqe_stats* stats);
 
+/* ---------------------------------------------------------------- noise trajectories */
+
+/* One channel placement of a NoisyCircuit (src/QuantumMatter.Core/Noise/NoisyCircuit.cs:38-48):
+ * kind is NoiseKind (0 bit flip, 1 phase flip, 2 depolarizing, 3 amplitude damping,
+ * Noise/NoiseChannel.cs:4-14), the channel acts after the first `position` gates. */
+typedef struct qm_channel {
+    int32_t kind;
+    int32_t target;
+    double probability;
+    int32_t position;
+    int32_t reserved;
+} qm_channel;                /* 24 bytes */
+
+/* Per-trajectory outputs of qm_trajectories_run; every pointer may be NULL. */
+typedef struct qm_trajectory_outputs {
+    double* values;              /* [trajectories][term_count]: <P_t> / mass at the end */
+    double* masses;              /* [trajectories]: final Born mass */
+    int32_t* consumed;           /* [trajectories]: draws consumed (the measurement's included) */
+    int8_t* branches;            /* [trajectories][channel_count]: -1 skipped (p == 0), Pauli
+                                    0..3 = I/X/Y/Z, damping 0 = stay, 1 = jump */
+    int32_t* ambiguous;          /* [trajectories]: damping selections whose draw lay within the
+                                    rounding margin of jumpMass / total */
+    int64_t* outcomes;           /* [trajectories]: StateVector.MeasureAll of the final state with
+                                    the trajectory's next draw (NoisyStateVectorSimulator.Run) */
+    double* probability_means;   /* [2^qubits]: Welford mean of |psi_i|^2 / mass over trajectories */
+    double* probability_stderr;  /* [2^qubits]: sqrt(M2 / (T (T - 1)))
+                                    (NoisyStateVectorSimulator.EstimateProbabilities) */
+} qm_trajectory_outputs;
+
+typedef struct qm_trajectory_stats {
+    int32_t segments;            /* fused schedules between damping decisions */
+    int32_t passes;              /* fused passes per trajectory */
+    int32_t mass_passes;         /* joint-mass (histogram) passes per trajectory */
+    int32_t waves;
+    int32_t batch_states;
+    int32_t reserved;
+    double device_seconds;
+    double wall_seconds;
+} qm_trajectory_stats;
+
+/* NoisyCircuit.Execute for `trajectories` independent trajectories at once
+ * (NoisyStateVectorSimulator.cs:36-106, CpuNoiseChannelBackend.cs:10-145).  Every trajectory
+ * starts from |0...0>, runs the prepared gates with the channel placements between them and
+ * consumes its own draws, draws[t * draw_stride + k], in the reference's order: one per
+ * depolarizing placement, one per flip unless p == 1, one per damping unless the jump or the
+ * stay branch has zero mass, none for p == 0, then one for the measurement when `outcomes` is
+ * requested.  Branch selection follows the reference's thresholds on the given draws; damping
+ * renormalisation uses FP64 masses.  QM_E_RANGE when a trajectory needs more than draw_stride
+ * draws, QM_E_MASS when a damping meets no finite positive mass.  stats may be NULL. */
+int32_t qm_trajectories_run(qm_context* context, int32_t qubits, int32_t precision, const qm_gate* gates,
+                            int32_t gate_count, const qm_channel* channels, int32_t channel_count,
+                            int32_t trajectories, const double* draws, int32_t draw_stride,
+                            const qm_pauli_term* terms, int32_t term_count, const qm_trajectory_outputs* outputs,
+                            qm_trajectory_stats* stats);
+
+/* The NextDouble() stream of a seeded System.Random (the reference's draw source for
+ * measurements and Kraus selectors, NoisyStateVectorSimulator.cs:111): values skip .. skip +
+ * count - 1 of Random(seed). */
+int32_t qm_random_doubles(int32_t seed, int64_t skip, int64_t count, double* out);
+
 /* ---------------------------------------------------------------- allocation-free expectation */
 
 /* No counterpart in the reference: an additive entry point for hosts that cannot allocate

@@ -38,6 +38,11 @@ class Random(C.Structure):
     _fields_ = [("seed_array", C.c_int32 * 56), ("inext", C.c_int32), ("inextp", C.c_int32)]
 
 
+class Channel(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("target", C.c_int32), ("probability", C.c_double),
+                ("position", C.c_int32), ("reserved", C.c_int32)]
+
+
 _lib = None
 
 
@@ -79,6 +84,8 @@ def load() -> C.CDLL:
     lib.qmo_random_next_double.restype = C.c_double
     lib.qmp_execute.argtypes = [C.POINTER(ParallelOptions), C.POINTER(Op), C.c_int32, C.c_int32, C.c_void_p]
     lib.qmp_hardware_threads.restype = C.c_int32
+    lib.qmo_trajectory.argtypes = [C.POINTER(Op), C.c_int32, C.POINTER(Channel), C.c_int32, C.c_int32, C.c_void_p,
+                                   DP, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int8)]
     _lib = lib
     return lib
 
@@ -192,6 +199,26 @@ def noise_apply(kind: int, p: float, target: int, state: np.ndarray, draws: Sequ
     if rc:
         raise RuntimeError(f"oracle noise failed: {rc}")
     return s, used.value
+
+
+def trajectory(noisy_circuit, draws: Sequence[float]) -> tuple[np.ndarray, int, np.ndarray]:
+    """One NoisyCircuit.Execute trajectory from |0...0> with the given draws.
+    Returns (final state, draws consumed, branch per placement)."""
+    flat, placements = noisy_circuit.Flatten()
+    ops, n = ops_array(flat.Operations)
+    ch = (Channel * max(1, len(placements)))()
+    for i, (c, target, pos) in enumerate(placements):
+        ch[i].kind, ch[i].target, ch[i].probability, ch[i].position = int(c.Kind), target, c.Probability, pos
+    s = zero_state(noisy_circuit.QubitCount)
+    d = np.ascontiguousarray(draws, dtype=np.float64)
+    dbuf = d.ctypes.data_as(C.POINTER(C.c_double)) if d.size else None
+    used = C.c_int32()
+    branches = np.full(max(1, len(placements)), -1, dtype=np.int8)
+    rc = load().qmo_trajectory(ops, n, ch, len(placements), noisy_circuit.QubitCount, _buf(s), dbuf, int(d.size),
+                               C.byref(used), branches.ctypes.data_as(C.POINTER(C.c_int8)))
+    if rc:
+        raise RuntimeError(f"oracle trajectory failed: {rc}")
+    return s, used.value, branches[:len(placements)]
 
 
 def qubit_masses(state: np.ndarray, target: int) -> tuple[float, float]:

@@ -325,12 +325,14 @@ void qmo_qubit_masses(const double* s, int32_t qubits, int32_t target, double* m
 }
 
 /* CpuNoiseChannelBackend.Apply / ApplyDamping (src/QuantumMatter.Infrastructure/CpuNoiseChannelBackend.cs:10-145) */
-int qmo_noise_apply(int32_t kind, double p, int32_t target, double* s, int32_t qubits,
-                    const double* draws, int32_t ndraws, int32_t* used) {
+/* *branch: -1 for p == 0 (nothing happens), Pauli 0..3 = I, X, Y, Z, damping 0 = stay, 1 = jump. */
+static int noise_apply(int32_t kind, double p, int32_t target, double* s, int32_t qubits, const double* draws,
+                       int32_t ndraws, int32_t* used, int32_t* branch) {
     int64_t len = (int64_t)1 << qubits, bit = (int64_t)1 << target;
     int32_t consumed = 0;
 #define NEXT_DRAW() (consumed < ndraws ? draws[consumed++] : (consumed++, 0.0))
     if (used) *used = 0;
+    *branch = -1;
     if (p == 0) return 0;
     if (kind == 3) {
         double zero_mass, one_mass;
@@ -340,8 +342,9 @@ int qmo_noise_apply(int32_t kind, double p, int32_t target, double* s, int32_t q
         double total = jump_mass + stay_mass;
         if (!isfinite(total) || total <= 0) return 7;
         int jump = jump_mass > 0 && (stay_mass == 0 || NEXT_DRAW() < jump_mass / total);
-        double branch = jump ? jump_mass : stay_mass;
-        double scale = 1 / sqrt(branch);
+        *branch = jump;
+        double branch_mass = jump ? jump_mass : stay_mass;
+        double scale = 1 / sqrt(branch_mass);
         double jump_scale = sqrt(p) * scale;
         double stay_scale = sqrt(1 - p) * scale;
         for (int64_t pair = 0; pair < len / 2; ++pair) {
@@ -371,6 +374,7 @@ int qmo_noise_apply(int32_t kind, double p, int32_t target, double* s, int32_t q
         pauli = !apply ? 0 : kind == 0 ? 1 : 3;
     }
     if (used) *used = consumed;
+    *branch = pauli;
     if (pauli == 0) return 0;
     for (int64_t pair = 0; pair < len / 2; ++pair) {
         int64_t low = pair & (bit - 1);
@@ -386,6 +390,44 @@ int qmo_noise_apply(int32_t kind, double p, int32_t target, double* s, int32_t q
     }
     return 0;
 #undef NEXT_DRAW
+}
+
+int qmo_noise_apply(int32_t kind, double p, int32_t target, double* s, int32_t qubits,
+                    const double* draws, int32_t ndraws, int32_t* used) {
+    int32_t branch;
+    return noise_apply(kind, p, target, s, qubits, draws, ndraws, used, &branch);
+}
+
+/* One trajectory of NoisyCircuit.Execute (src/QuantumMatter.Core/Noise/NoisyCircuit.cs:48-65)
+ * through CpuStateVectorBackend and CpuNoiseChannelBackend: the operations run in order and
+ * channel j is applied after the first channels[j].position operations; p == 0 placements
+ * are skipped without a draw.  Draws are consumed from `draws` in order; *used receives the
+ * count (it may exceed ndraws, in which case the missing draws read as 0).  branches (may be
+ * NULL) receives one entry per channel (see noise_apply). */
+int qmo_trajectory(const qmo_operation* ops, int32_t count, const qmo_channel* channels, int32_t nch,
+                   int32_t qubits, double* amps, const double* draws, int32_t ndraws, int32_t* used,
+                   int8_t* branches) {
+    int32_t done = 0, consumed = 0;
+    for (int32_t j = 0; j < nch; ++j) {
+        int32_t pos = channels[j].position;
+        if (pos < done || pos > count) return 1;
+        qmo_execute(ops + done, pos - done, qubits, amps);
+        done = pos;
+        int32_t step = 0, branch = -1;
+        const double* rest = consumed < ndraws ? draws + consumed : draws;
+        int32_t left = consumed < ndraws ? ndraws - consumed : 0;
+        int rc = noise_apply(channels[j].kind, channels[j].probability, channels[j].target, amps, qubits, rest,
+                             left, &step, &branch);
+        if (rc) {
+            if (used) *used = consumed;
+            return rc;
+        }
+        consumed += step;
+        if (branches) branches[j] = (int8_t)branch;
+    }
+    qmo_execute(ops + done, count - done, qubits, amps);
+    if (used) *used = consumed;
+    return 0;
 }
 
 /* ---------------------------------------------------------------- sampling */

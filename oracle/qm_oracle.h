@@ -81,6 +81,19 @@ int qmo_noise_apply(int32_t kind, double p, int32_t target, double* amps, int32_
                     const double* draws, int32_t ndraws, int32_t* used);
 void qmo_qubit_masses(const double* amps, int32_t qubits, int32_t target, double* m0, double* m1);
 
+/* One channel placement of a NoisyCircuit: NoiseKind, target, probability, and the number of
+ * operations that precede it (Noise/NoisyCircuit.cs:38-48).  Same layout as qm_channel. */
+typedef struct qmo_channel {
+    int32_t kind;
+    int32_t target;
+    double probability;
+    int32_t position;
+    int32_t reserved;
+} qmo_channel;
+int qmo_trajectory(const qmo_operation* ops, int32_t count, const qmo_channel* channels, int32_t nch,
+                   int32_t qubits, double* amps, const double* draws, int32_t ndraws, int32_t* used,
+                   int8_t* branches);
+
 /* ---- sampling ---- */
 int qmo_sample(const double* amps, int32_t qubits, const double* draws, int32_t shots, int64_t* out);
 int qmo_measure_all(double* amps, int32_t qubits, double draw, int64_t* outcome);

@@ -76,6 +76,24 @@ class VqeStats(C.Structure):
                 ("wall_seconds", C.c_double)]
 
 
+class ChannelC(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("target", C.c_int32), ("probability", C.c_double),
+                ("position", C.c_int32), ("reserved", C.c_int32)]
+
+
+class TrajectoryOutputs(C.Structure):
+    _fields_ = [("values", C.POINTER(C.c_double)), ("masses", C.POINTER(C.c_double)),
+                ("consumed", C.POINTER(C.c_int32)), ("branches", C.POINTER(C.c_int8)),
+                ("ambiguous", C.POINTER(C.c_int32)), ("outcomes", C.POINTER(C.c_int64)),
+                ("probability_means", C.POINTER(C.c_double)), ("probability_stderr", C.POINTER(C.c_double))]
+
+
+class TrajectoryStats(C.Structure):
+    _fields_ = [("segments", C.c_int32), ("passes", C.c_int32), ("mass_passes", C.c_int32),
+                ("waves", C.c_int32), ("batch_states", C.c_int32), ("reserved", C.c_int32),
+                ("device_seconds", C.c_double), ("wall_seconds", C.c_double)]
+
+
 NEXT_DOUBLE_FN = C.CFUNCTYPE(C.c_double, C.c_void_p)
 
 NOALLOC_MAX_TERMS = 64  # QM_NOALLOC_MAX_TERMS
@@ -129,6 +147,10 @@ SIGNATURES = {
     "qm_batch_expectation": (I32, [P, I32, C.POINTER(PauliTermC), I32, DP, DP]),
     "qm_vqe_evaluate": (I32, [P, I32, I32, C.POINTER(TemplateOp), I32, I32, C.POINTER(PauliTermC), I32, DP, I32, I32,
                               DP, DP, C.POINTER(VqeStats)]),
+    "qm_trajectories_run": (I32, [P, I32, I32, C.POINTER(Gate), I32, C.POINTER(ChannelC), I32, I32, DP, I32,
+                                  C.POINTER(PauliTermC), I32, C.POINTER(TrajectoryOutputs),
+                                  C.POINTER(TrajectoryStats)]),
+    "qm_random_doubles": (I32, [I32, I64, I64, DP]),
     "qm_expectation_pauli_noalloc": (I32, [P, I32, I32, C.POINTER(PauliTermC), I32, DP, DP, P]),
 }
 

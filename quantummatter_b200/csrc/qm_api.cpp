@@ -223,6 +223,10 @@ int32_t validate_gates(const qm_gate* gates, int32_t count, int32_t qubits) {
 
 namespace qm {
 
+int32_t validate_prepared_gates(const qm_gate* gates, int32_t count, int32_t qubits) {
+    return validate_gates(gates, count, qubits);
+}
+
 int32_t plan_upload(Plan& plan, cudaStream_t stream, void** buffer, size_t* buffer_bytes) {
     if (plan.ops.empty() || plan.d_ops) return QM_OK;
     const size_t bytes = plan.ops.size() * sizeof(FusedOp);
@@ -1098,6 +1102,17 @@ int32_t device_sample(qm_state* st, const double* draws, int32_t shots, int64_t*
 }
 
 }  // namespace
+
+int32_t qm_sample_amplitudes(qm_context* ctx, void* amps, int32_t qubits, int32_t precision, const double* draws,
+                             int32_t shots, int64_t* outcomes, int32_t* ambiguous) {
+    qm_state view;
+    view.ctx = ctx;
+    view.qubits = qubits;
+    view.precision = precision;
+    view.amps = amps;
+    view.bytes = (precision == QM_FP32 ? 8ll : 16ll) << qubits;
+    return device_sample(&view, draws, shots, outcomes, ambiguous);
+}
 
 extern "C" int32_t qm_sample(qm_state* st, const double* draws, int32_t shots, int64_t* outcomes, int32_t* ambiguous) {
     int32_t rc = check_state(st);

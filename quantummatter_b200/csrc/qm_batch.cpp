@@ -123,6 +123,17 @@ bool plan_tiles(int qubits, int precision, const qm_pauli_term* terms, int count
     return true;
 }
 
+cudaError_t enqueue_tile_expectation(const void* amps, int qubits, int precision, const TilePlan& tp, int states,
+                                     double* partials, double* out, cudaStream_t st) {
+    const size_t partial = sizeof(double) * (size_t)states * tp.rows_per_state * tp.columns;
+    cudaError_t e = cudaMemsetAsync(partials, 0, partial, st);
+    for (size_t i = 0; e == cudaSuccess && i < tp.passes.size(); ++i)
+        e = launch_expect_tile(amps, qubits, precision, tp.passes[i], tp.terms.data(), states, (uint64_t)1 << qubits,
+                               partials, tp.columns, tp.rows_per_state, tp.mass_column, st);
+    if (e == cudaSuccess) e = launch_finish_batched(partials, states, tp.rows_per_state, tp.columns, out, st);
+    return e;
+}
+
 }  // namespace qm
 
 namespace {
@@ -161,11 +172,7 @@ int32_t enqueue_tiles(qm_batch* b, const TilePlan& tp, int states, cudaStream_t 
     if (rc) return rc;
     rc = grow(b->out, b->out_bytes, sizeof(double) * (size_t)states * tp.columns);
     if (rc) return rc;
-    QM_CUDA(cudaMemsetAsync(b->partials, 0, partial, st));
-    for (const TilePass& p : tp.passes)
-        QM_CUDA(launch_expect_tile(b->amps, b->qubits, b->precision, p, tp.terms.data(), states, (uint64_t)1 << b->qubits,
-                                   b->partials, tp.columns, tp.rows_per_state, tp.mass_column, st));
-    QM_CUDA(launch_finish_batched(b->partials, states, tp.rows_per_state, tp.columns, b->out, st));
+    QM_CUDA(enqueue_tile_expectation(b->amps, b->qubits, b->precision, tp, states, b->partials, b->out, st));
     return QM_OK;
 }
 

@@ -120,6 +120,44 @@ __device__ __forceinline__ void op_matrix_any(Cx<T> (&a)[NR], const FusedOp& op,
     }
 }
 
+template <typename T, int M>
+__device__ __forceinline__ void op_scale(Cx<T> (&a)[NR], T s0, T s1) {
+#pragma unroll
+    for (int i = 0; i < NR; ++i) {
+        const T s = ((i >> M) & 1) ? s1 : s0;
+        a[i].re *= s;
+        a[i].im *= s;
+    }
+}
+
+// A noise-branch op (kOpBranch, uncontrolled, target in register bit op.reg).  Its per-state
+// coefficients are mostly the identity (no Pauli error) or a real diagonal (a damping without
+// a jump, a Z error); the test is uniform across the CTA, which works on one state.
+template <typename T>
+__device__ __forceinline__ void op_branch(Cx<T> (&a)[NR], const FusedOp& op, const Coef& c, const Layout& L) {
+    const bool real = c.v[1] == 0 && c.v[3] == 0 && c.v[5] == 0 && c.v[7] == 0;
+    if (!real) {
+        op_matrix_any<T, false, false>(a, op, c, L);
+        return;
+    }
+    if (c.v[2] != 0 || c.v[4] != 0) {
+        op_matrix_any<T, true, false>(a, op, c, L);
+        return;
+    }
+    if (c.v[0] == 1 && c.v[6] == 1) return;
+    const T s0 = (T)c.v[0], s1 = (T)c.v[6];
+    switch (op.reg) {
+    case 0: op_scale<T, 0>(a, s0, s1); break;
+    case 1: op_scale<T, 1>(a, s0, s1); break;
+#if QM_REG_BITS > 3
+    case 2: op_scale<T, 2>(a, s0, s1); break;
+    default: op_scale<T, 3>(a, s0, s1); break;
+#else
+    default: op_scale<T, 2>(a, s0, s1); break;
+#endif
+    }
+}
+
 // X on register bit M where the control lies outside the registers (or there is none):
 // a per-amplitude predicate.
 template <typename T, int M>
@@ -491,7 +529,8 @@ __global__ void __launch_bounds__(1 << (K - R), ((sizeof(T) == 8 && K == 12) || 
             }
             switch (code) {
             case OP_MATRIX:
-                if (ctrl) op_matrix_any<T, false, true>(a, op, c, L);
+                if (op.flags & kOpBranch) op_branch<T>(a, op, c, L);
+                else if (ctrl) op_matrix_any<T, false, true>(a, op, c, L);
                 else op_matrix_any<T, false, false>(a, op, c, L);
                 break;
             case OP_MATRIX_REAL:
@@ -544,10 +583,11 @@ cudaError_t launch_k(void* amps, int qubits, const FusedPass& p, const FusedOp* 
     L.ops = d_ops + p.op_begin;
     L.cta_shift = qubits - K;
     L.states = batch ? batch->states : 1;
-    L.table = batch ? batch->table : nullptr;
+    const bool tabled = batch && batch->table;
+    L.table = tabled ? batch->table + 8 * (size_t)batch->slot_offset : nullptr;
     L.state_stride = batch ? batch->state_stride : 0;
     L.table_stride = batch ? batch->table_stride : 0;
-    L.table_slots = (batch && batch->table) ? (int32_t)(batch->table_stride / 8) : 0;
+    L.table_slots = !tabled ? 0 : batch->slot_count >= 0 ? batch->slot_count : (int32_t)(batch->table_stride / 8);
     L.pad = 0;
     const size_t smem = tile_bytes<T, K>() + program_bytes(p.op_count) + sizeof(double) * 8 * (size_t)L.table_slots;
     static int optin = 0, sms = 0;

@@ -39,6 +39,8 @@ struct DevGate {
     double a[2], b[2], c[2], d[2];
 };
 DevGate to_dev_gate(const qm_gate& g);
+// Kernel ids, qubit ranges, control/target overlap and finite coefficients of prepared gates.
+int32_t validate_prepared_gates(const qm_gate* gates, int32_t count, int32_t qubits);
 
 // ---------------------------------------------------------------- fused-pass program
 // One fused pass touches a block of 2^k amplitudes per CTA: the local index bits are
@@ -57,6 +59,10 @@ constexpr int kMaxPassOps = 256;    // ops per pass: the program (88 B per op) i
 constexpr int kMaxPassGates = 120;  // gates absorbed per pass (stage changes add at most gates + 2)
 
 constexpr uint16_t kOpTable = 4;    // FusedOp::flags: coefficients come from the batch's table
+constexpr uint16_t kOpBranch = 8;   // FusedOp::flags: a table op realising a noise branch; the kernel
+                                    // skips identities and applies real diagonals as scalings
+// A coefficient slot passed to plan_fused with this bit set marks a noise-branch op (kOpBranch).
+constexpr int32_t kSlotBranch = 1 << 24;
 
 enum OpCode : uint8_t {
     OP_STAGE = 0,       // new register layout: reg_pos[0..R) local bit positions
@@ -123,11 +129,15 @@ int default_block_qubits(int qubits, int precision);
 cudaError_t launch_gate(void* amps, int qubits, int precision, const DevGate& g, cudaStream_t s);
 // A batch of equally sized states with one shared plan: state b at amps + b * state_stride
 // (elements); ops flagged kOpTable read 8 coefficients at table + b * table_stride + 8 * op.reserved.
+// With slot_count >= 0 a pass stages only slots [slot_offset, slot_offset + slot_count) of each
+// row and op.reserved counts from slot_offset.
 struct FusedBatch {
     int32_t states;
     uint64_t state_stride;
     const double* table;
     uint64_t table_stride;
+    int32_t slot_offset = 0;
+    int32_t slot_count = -1;
 };
 cudaError_t launch_fused(void* amps, int qubits, int precision, const FusedPass& p, const FusedOp* ops,
                          const FusedBatch* batch, cudaStream_t s);
@@ -192,8 +202,57 @@ cudaError_t launch_expect_tile(const void* amps, int qubits, int precision, cons
 cudaError_t launch_finish_batched(const double* partials, int states, int rows, int columns, double* out,
                                   cudaStream_t s);
 cudaError_t launch_reset_batched(void* amps, int qubits, int precision, int states, cudaStream_t s);
+// Tiled expectation of `states` states (stride 2^qubits) into out ([states][columns]: raw sums,
+// the mass in tp.mass_column); partials holds states * rows_per_state * columns doubles.
+cudaError_t enqueue_tile_expectation(const void* amps, int qubits, int precision, const TilePlan& tp, int states,
+                                     double* partials, double* out, cudaStream_t s);
+
+// ---------------------------------------------------------------- noise trajectories (qm_noise.cu)
+// Consecutive damping placements share one joint-mass histogram over their qubits (at most
+// kGroupMaxBits of them): bins[b] = sum of |psi_i|^2 over the i whose group bits spell b.
+constexpr int kGroupMaxBits = 8;
+constexpr int kGroupMaxBins = 1 << kGroupMaxBits;
+
+// One branch decision, taken per trajectory in program order on the device.
+struct Decision {
+    int32_t kind;     // NoiseKind: 0 bit flip, 1 phase flip, 2 depolarizing, 3 damping
+    int32_t channel;  // placement index (branch output column)
+    int32_t slot;     // coefficient slot (packed, per segment) of the op realising the branch
+    int32_t bit;      // damping: bit of the target in the group's histogram
+    double p;
+};
+int histogram_ctas(int qubits);
+// partials[state][cta][bin] for the group mask (global qubit bits, popcount <= kGroupMaxBits).
+cudaError_t launch_group_histogram(const void* amps, int qubits, int precision, int states, uint32_t group_mask,
+                                   double* partials, cudaStream_t s);
+struct DecideArgs {
+    const Decision* decisions;
+    int32_t count;
+    const double* partials;   // histogram partials of the group, or null when no damping is decided
+    int32_t ctas;             // partial rows per state
+    int32_t bins;
+    const double* draws;      // [states][draw_stride]
+    int32_t draw_stride;
+    int32_t* counters;        // draws consumed so far, per state
+    int32_t* status;          // per state: QM_OK, QM_E_RANGE (draws exhausted), QM_E_MASS
+    int32_t* ambiguous;       // per state
+    double* table;            // [states][table_stride]
+    uint64_t table_stride;    // doubles
+    int8_t* branches;         // [states][channels] or null
+    int32_t channels;
+    double margin;            // relative ambiguity margin of damping selections
+};
+cudaError_t launch_decide(const DecideArgs& a, int states, cudaStream_t s);
+// Welford update of mean/m2 over indices [0, len) with states first .. first+states-1 of the run.
+cudaError_t launch_welford(const void* amps, int precision, int states, uint64_t state_stride, int64_t len,
+                           const double* masses, int64_t first, double* mean, double* m2, cudaStream_t s);
+cudaError_t launch_welford_finish(double* m2, int64_t len, int64_t trajectories, cudaStream_t s);
 
 }  // namespace qm
+
+// Born-rule sampling of one state at a raw device address (qm_sample's engine).
+int32_t qm_sample_amplitudes(struct qm_context* ctx, void* amps, int32_t qubits, int32_t precision, const double* draws,
+                             int32_t shots, int64_t* outcomes, int32_t* ambiguous);
 
 // ---------------------------------------------------------------- handles
 struct qm_context {

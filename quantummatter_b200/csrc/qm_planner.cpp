@@ -140,6 +140,10 @@ bool plan_fused(const std::vector<qm_gate>& gates, int qubits, int precision, in
             error = "only matrix and diagonal gates can take per-state coefficients";
             return false;
         }
+        if (slot >= 0 && (slot & kSlotBranch) && (g.kernel != QM_KERNEL_MATRIX || g.control_mask != 0)) {
+            error = "a noise branch is an uncontrolled matrix placeholder";
+            return false;
+        }
         GInfo info = classify(g);
         info.slot = slot;
         remaining.push_back(info);
@@ -327,7 +331,13 @@ bool plan_fused(const std::vector<qm_gate>& gates, int qubits, int precision, in
                 std::memcpy(&op.coef[2], g.b, 16);
                 std::memcpy(&op.coef[4], g.c, 16);
                 std::memcpy(&op.coef[6], g.d, 16);
-                if (gi.slot >= 0) {
+                if (gi.slot >= 0 && (gi.slot & kSlotBranch)) {
+                    // noise branch: per-state coefficients, tested at run time
+                    op.flags = kOpTable | kOpBranch;
+                    op.reserved = (uint32_t)(gi.slot & (kSlotBranch - 1));
+                    op.code = OP_MATRIX;
+                    op.reg = (int8_t)reg_of_local[local_of[g.target]];
+                } else if (gi.slot >= 0) {
                     // per-state coefficients: generic op reading the batch table
                     op.flags = kOpTable;
                     op.reserved = (uint32_t)gi.slot;

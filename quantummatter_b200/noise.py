@@ -86,3 +86,31 @@ class NoisyCircuit:
             raise ArgumentOutOfRangeError("target")
         self._steps.append(NoisyStep(None, channel, target))
         return self
+
+    def Flatten(self) -> tuple[QuantumCircuit, list[tuple[NoiseChannel, int, int]]]:
+        """All unitary segments as one circuit, plus (channel, target, position) placements, where
+        a placement acts after the first `position` operations (the order NoisyCircuit.Execute
+        applies them in)."""
+        flat = QuantumCircuit(self.QubitCount)
+        placements: list[tuple[NoiseChannel, int, int]] = []
+        count = 0
+        for step in self._steps:
+            if step.Circuit is not None:
+                for op in step.Circuit.Operations:
+                    flat.AppendValidated(op)
+                    count += 1
+            else:
+                placements.append((step.Channel, step.Target, count))
+        return flat, placements
+
+    def MaxDraws(self) -> int:
+        """Draws one trajectory can consume: every placement with p > 0 except certain flips."""
+        n = 0
+        for step in self._steps:
+            ch = step.Channel
+            if ch is None or ch.Probability == 0:
+                continue
+            if ch.Kind in (NoiseKind.BitFlip, NoiseKind.PhaseFlip) and ch.Probability == 1:
+                continue
+            n += 1
+        return n
