@@ -120,3 +120,30 @@ def uniform_parameters(count: int, vectors: int, lo: float, hi: float, seed: int
     import numpy as np
     rng = SplitMix64(seed)
     return np.array([[rng.uniform(lo, hi) for _ in range(count)] for _ in range(vectors)], dtype=np.float64)
+
+
+def noisy_ry_cz_ladder(qubits: int, depth: int, seed: int = DEFAULT_SEED, p1: float = 1e-3, p2: float = 1e-2,
+                       gamma: float = 1e-3):
+    """Noisy RY / CZ-ladder circuit of the trajectory workload.
+
+    Each layer: RY(theta ~ U[0, 2pi)) on every qubit, each followed by depolarizing(p1) on its
+    qubit; then CZ(i, i+1) for i = 0..n-2, each followed by depolarizing(p2) on both of its
+    qubits; then amplitude damping(gamma) on every qubit.  24 qubits x 30 layers gives
+    30 x (24 + 23) = 1410 gates and 30 x (24 + 46 + 24) = 2820 channel placements.
+    """
+    from .noise import NoiseChannel, NoisyCircuit
+    rng = SplitMix64(seed)
+    nc = NoisyCircuit(qubits)
+    dep1, dep2, damp = NoiseChannel.Depolarizing(p1), NoiseChannel.Depolarizing(p2), NoiseChannel.AmplitudeDamping(gamma)
+    two_pi = 2 * math.pi
+    for _ in range(depth):
+        for q in range(qubits):
+            nc.Append(QuantumCircuit(qubits).Ry(q, rng.uniform(0, two_pi)))
+            nc.ApplyNoise(dep1, q)
+        for q in range(qubits - 1):
+            nc.Append(QuantumCircuit(qubits).CZ(q, q + 1))
+            nc.ApplyNoise(dep2, q)
+            nc.ApplyNoise(dep2, q + 1)
+        for q in range(qubits):
+            nc.ApplyNoise(damp, q)
+    return nc
