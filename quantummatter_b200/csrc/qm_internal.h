@@ -213,13 +213,36 @@ cudaError_t enqueue_tile_expectation(const void* amps, int qubits, int precision
 constexpr int kGroupMaxBits = 8;
 constexpr int kGroupMaxBins = 1 << kGroupMaxBits;
 
-// One branch decision, taken per trajectory in program order on the device.
+// Every trajectory carries a Pauli frame F = X^fx Z^fz: its true state is F applied to the stored
+// state (up to a global phase).  Pauli errors and Pauli gates only update the frame, Clifford
+// gates run unchanged and conjugate the frame, and every other gate or Kraus operator U runs as
+// F U F on the stored state (per-trajectory coefficients in the batch table).
+enum StepKind : int32_t {
+    STEP_PAULI_BIT_FLIP = 0,    // NoiseKind values: a channel decision from one draw
+    STEP_PAULI_PHASE_FLIP = 1,
+    STEP_PAULI_DEPOLARIZING = 2,
+    STEP_DAMPING = 3,           // a Kraus selection on the group's joint masses
+    STEP_FRAME_X = 10,          // Pauli gate or certain flip on qubit a
+    STEP_FRAME_Y = 11,
+    STEP_FRAME_Z = 12,
+    STEP_FRAME_H = 13,          // Clifford gates (they also run on the stored state)
+    STEP_FRAME_S = 14,
+    STEP_FRAME_CNOT = 15,       // control b, target a
+    STEP_FRAME_CZ = 16,
+    STEP_FRAME_SWAP = 17,
+    STEP_CONJ = 20,             // write F U F (U = coef) for the gate on qubit a into `slot`
+    STEP_FLUSH_X = 21,          // apply the frame's X on qubit a to the stored state (X or I into `slot`)
+};
+
+// One step of a trajectory's program, taken per trajectory in program order on the device.
 struct Decision {
-    int32_t kind;     // NoiseKind: 0 bit flip, 1 phase flip, 2 depolarizing, 3 damping
-    int32_t channel;  // placement index (branch output column)
-    int32_t slot;     // coefficient slot (packed, per segment) of the op realising the branch
+    int32_t kind;     // StepKind
+    int32_t channel;  // placement index (branch output column), -1 for gate steps
+    int32_t slot;     // coefficient slot (packed, per segment) written by the step, -1 for none
     int32_t bit;      // damping: bit of the target in the group's histogram
+    int32_t a, b;     // qubits: target (a) and control or second operand (b)
     double p;
+    double coef[8];   // STEP_CONJ: the gate's a, b, c, d
 };
 int histogram_ctas(int qubits);
 // partials[state][cta][bin] for the group mask (global qubit bits, popcount <= kGroupMaxBits).
@@ -241,11 +264,19 @@ struct DecideArgs {
     int8_t* branches;         // [states][channels] or null
     int32_t channels;
     double margin;            // relative ambiguity margin of damping selections
+    uint32_t group_mask;      // qubits of the histogram group (damping steps)
+    uint32_t* frame_x;        // per state Pauli frame
+    uint32_t* frame_z;
 };
 cudaError_t launch_decide(const DecideArgs& a, int states, cudaStream_t s);
-// Welford update of mean/m2 over indices [0, len) with states first .. first+states-1 of the run.
+// Welford update of mean/m2 over indices [0, len) with states first .. first+states-1 of the run;
+// state b's true probability at i is the stored one at i ^ frame_x[b].
 cudaError_t launch_welford(const void* amps, int precision, int states, uint64_t state_stride, int64_t len,
-                           const double* masses, int64_t first, double* mean, double* m2, cudaStream_t s);
+                           const double* masses, const uint32_t* frame_x, int64_t first, double* mean, double* m2,
+                           cudaStream_t s);
+// Applies X^frame_x[b] to every state b in place (pair swaps).
+cudaError_t launch_frame_flip(void* amps, int qubits, int precision, int states, const uint32_t* frame_x,
+                              cudaStream_t s);
 cudaError_t launch_welford_finish(double* m2, int64_t len, int64_t trajectories, cudaStream_t s);
 
 }  // namespace qm

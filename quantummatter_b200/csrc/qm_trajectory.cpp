@@ -56,15 +56,38 @@ struct Program {
     }
 };
 
-qm_gate prepared_pauli(int kind, int target) {
-    qm_operation o{};
-    o.kind = kind;
-    o.target = target;
-    o.control = -1;
-    o.second_control = -1;
-    qm_gate g{};
-    qm_prepare_gates(&o, 1, target + 1, &g);
-    return g;
+enum GateClass { GC_SKIP, GC_X, GC_Y, GC_Z, GC_H, GC_S, GC_CNOT, GC_CZ, GC_SWAP, GC_OTHER };
+
+// Pauli and Clifford gates recognised from their prepared records (exact coefficients only).
+GateClass classify_gate(const qm_gate& g) {
+    auto is = [](const double* v, double re, double im) { return v[0] == re && v[1] == im; };
+    const int controls = __builtin_popcount(g.control_mask);
+    switch (g.kernel) {
+    case QM_KERNEL_IDENTITY: return GC_SKIP;
+    case QM_KERNEL_EXCHANGE: return controls == 0 ? GC_X : controls == 1 ? GC_CNOT : GC_OTHER;
+    case QM_KERNEL_SWAP: return controls == 0 ? GC_SWAP : GC_OTHER;
+    case QM_KERNEL_HADAMARD: return controls == 0 ? GC_H : GC_OTHER;
+    case QM_KERNEL_DIAGONAL:
+        if (is(g.a, 1, 0) && is(g.d, 1, 0)) return GC_SKIP;
+        if (is(g.a, 1, 0) && is(g.d, -1, 0)) return controls == 0 ? GC_Z : controls == 1 ? GC_CZ : GC_OTHER;
+        if (controls == 0 && is(g.a, 1, 0) && (is(g.d, 0, 1) || is(g.d, 0, -1))) return GC_S;
+        return GC_OTHER;
+    case QM_KERNEL_MATRIX:
+        if (controls == 0 && is(g.a, 0, 0) && is(g.b, 0, -1) && is(g.c, 0, 1) && is(g.d, 0, 0)) return GC_Y;
+        return GC_OTHER;
+    default: return GC_OTHER;
+    }
+}
+
+Decision step(int32_t kind, int32_t a, int32_t b = -1) {
+    Decision d{};
+    d.kind = kind;
+    d.channel = -1;
+    d.slot = -1;
+    d.bit = 0;
+    d.a = a;
+    d.b = b;
+    return d;
 }
 
 // The fused schedule's placeholder for a noise branch; its coefficients come from the table.
@@ -83,20 +106,22 @@ int32_t compile(const qm_gate* gates, int32_t gate_count, const qm_channel* ch, 
                 int32_t exec_qubits, int32_t precision, Program& P) {
     P.fixed.assign((size_t)nch, -1);
     Segment cur;
-    bool open = false;
+    bool open = false;  // a run of dampings is open: its steps wait for the joint masses
     uint32_t mask = 0;
-    std::vector<Decision> pending;  // dampings of the open group (bit = target until closed)
+    std::vector<Decision> pending;  // steps of the open run, in program order
+    auto add_step = [&](const Decision& d) { (open ? pending : cur.decisions).push_back(d); };
     auto close_group = [&]() {
         P.groups.push_back(mask);
         cur.group = (int32_t)P.groups.size() - 1;
         P.segments.push_back(std::move(cur));
         cur = Segment();
         for (Decision d : pending) {
-            const int target = d.bit;
-            d.bit = __builtin_popcount(mask & ((1u << target) - 1u));
-            d.slot = cur.local_slots++;
-            cur.gates.push_back(branch_placeholder(target));
-            cur.slots.push_back(d.slot | kSlotBranch);
+            if (d.kind == STEP_DAMPING) {
+                d.bit = __builtin_popcount(mask & ((1u << d.a) - 1u));
+                d.slot = cur.local_slots++;
+                cur.gates.push_back(branch_placeholder(d.a));
+                cur.slots.push_back(d.slot | kSlotBranch);
+            }
             cur.decisions.push_back(d);
         }
         P.max_bins = std::max(P.max_bins, 1 << __builtin_popcount(mask));
@@ -104,13 +129,62 @@ int32_t compile(const qm_gate* gates, int32_t gate_count, const qm_channel* ch, 
         open = false;
         mask = 0;
     };
-    int32_t done = 0;
-    auto gates_until = [&](int32_t pos) {
-        for (; done < pos; ++done) {
-            if (open) close_group();
-            cur.gates.push_back(gates[done]);
-            cur.slots.push_back(-1);
+    auto add_gate = [&](const qm_gate& g) -> int32_t {
+        const GateClass gc = classify_gate(g);
+        switch (gc) {
+        case GC_SKIP: return QM_OK;
+        case GC_X: add_step(step(STEP_FRAME_X, g.target)); return QM_OK;
+        case GC_Y: add_step(step(STEP_FRAME_Y, g.target)); return QM_OK;
+        case GC_Z: add_step(step(STEP_FRAME_Z, g.target)); return QM_OK;
+        default: break;
         }
+        if (open) close_group();
+        const int ctrl = g.control_mask ? __builtin_ctz(g.control_mask) : -1;
+        if (gc != GC_OTHER) {  // a Clifford gate: runs unchanged, conjugates the frame
+            cur.gates.push_back(g);
+            cur.slots.push_back(-1);
+            const int32_t kind = gc == GC_H ? STEP_FRAME_H : gc == GC_S ? STEP_FRAME_S : gc == GC_CNOT ? STEP_FRAME_CNOT
+                                 : gc == GC_CZ ? STEP_FRAME_CZ : STEP_FRAME_SWAP;
+            cur.decisions.push_back(step(kind, g.target, gc == GC_SWAP ? g.swap_control : ctrl));
+            return QM_OK;
+        }
+        if (g.kernel == QM_KERNEL_SWAP) return fail(QM_E_UNSUPPORTED, "controlled swap is not a reference gate");
+        // the frame's X on a control would turn "control on one" into "control on zero": apply it first
+        for (int q = 0; q < 32; ++q)
+            if (g.control_mask & (1u << q)) {
+                Decision f = step(STEP_FLUSH_X, q);
+                f.slot = cur.local_slots++;
+                cur.gates.push_back(branch_placeholder(q));
+                cur.slots.push_back(f.slot | kSlotBranch);
+                cur.decisions.push_back(f);
+            }
+        qm_gate ph = g;
+        if (g.kernel == QM_KERNEL_EXCHANGE) {  // Toffoli: X on the target as a matrix
+            ph.kernel = QM_KERNEL_MATRIX;
+            ph.a[0] = ph.a[1] = ph.b[1] = ph.c[1] = ph.d[0] = ph.d[1] = 0.0;
+            ph.b[0] = ph.c[0] = 1.0;
+        } else if (g.kernel == QM_KERNEL_HADAMARD) {
+            ph.kernel = QM_KERNEL_MATRIX;
+        }
+        Decision c = step(STEP_CONJ, g.target);
+        c.slot = cur.local_slots++;
+        std::memcpy(&c.coef[0], ph.a, 16);
+        std::memcpy(&c.coef[2], ph.b, 16);
+        std::memcpy(&c.coef[4], ph.c, 16);
+        std::memcpy(&c.coef[6], ph.d, 16);
+        cur.gates.push_back(ph);
+        cur.slots.push_back(c.slot);
+        cur.decisions.push_back(c);
+        return QM_OK;
+    };
+    int32_t done = 0;
+    int32_t rc = QM_OK;
+    auto gates_until = [&](int32_t pos) -> int32_t {
+        for (; done < pos; ++done) {
+            int32_t r = add_gate(gates[done]);
+            if (r) return r;
+        }
+        return QM_OK;
     };
     int32_t last = 0;
     for (int32_t j = 0; j < nch; ++j) {
@@ -122,33 +196,34 @@ int32_t compile(const qm_gate* gates, int32_t gate_count, const qm_channel* ch, 
         if (c.position < last || c.position > gate_count)
             return fail(QM_E_ARG, "channel positions must be nondecreasing and within the gate list");
         last = c.position;
-        gates_until(c.position);
+        if ((rc = gates_until(c.position))) return rc;
         if (c.probability == 0) continue;  // NoisyCircuit.Execute skips it without a draw
         if (c.kind == 3) {
             const uint32_t bit = 1u << c.target;
             if (open && !(mask & bit) && __builtin_popcount(mask) == kGroupMaxBits) close_group();
             open = true;
             mask |= bit;
-            pending.push_back(Decision{3, j, -1, c.target, c.probability});
+            Decision d = step(STEP_DAMPING, c.target);
+            d.channel = j;
+            d.p = c.probability;
+            pending.push_back(d);
             P.fixed[(size_t)j] = -2;
             ++P.max_draws;
             continue;
         }
-        if (open) close_group();
         if (c.kind != 2 && c.probability == 1) {  // a certain flip takes no draw
             P.fixed[(size_t)j] = (int8_t)(c.kind == 0 ? 1 : 3);
-            cur.gates.push_back(prepared_pauli(c.kind == 0 ? QM_GATE_X : QM_GATE_Z, c.target));
-            cur.slots.push_back(-1);
+            add_step(step(c.kind == 0 ? STEP_FRAME_X : STEP_FRAME_Z, c.target));
             continue;
         }
         P.fixed[(size_t)j] = -2;
         ++P.max_draws;
-        Decision d{c.kind, j, cur.local_slots++, 0, c.probability};
-        cur.gates.push_back(branch_placeholder(c.target));
-        cur.slots.push_back(d.slot | kSlotBranch);
-        cur.decisions.push_back(d);
+        Decision d = step(c.kind, c.target);
+        d.channel = j;
+        d.p = c.probability;
+        add_step(d);
     }
-    gates_until(gate_count);
+    if ((rc = gates_until(gate_count))) return rc;
     if (open) close_group();
     P.segments.push_back(std::move(cur));
 
@@ -176,7 +251,8 @@ int32_t compile(const qm_gate* gates, int32_t gate_count, const qm_channel* ch, 
         P.max_packed = std::max(P.max_packed, next);
         P.passes += (int32_t)s.plan.passes.size();
         for (Decision& d : s.decisions) {
-            if (packed_of[(size_t)d.slot] < 0) return fail(QM_E_DEVICE, "a noise branch was not scheduled");
+            if (d.slot < 0) continue;
+            if (packed_of[(size_t)d.slot] < 0) return fail(QM_E_DEVICE, "a per-trajectory op was not scheduled");
             d.slot = packed_of[(size_t)d.slot];
         }
         s.decision_offset = (int32_t)P.all_decisions.size();
@@ -253,7 +329,7 @@ extern "C" int32_t qm_trajectories_run(qm_context* ctx, int32_t qubits, int32_t 
     const int64_t state_bytes = (precision == QM_FP32 ? 8ll : 16ll) << n;
     const int64_t len = int64_t(1) << qubits;
     auto per_state = [&](int states) {
-        int64_t b = state_bytes + 64ll * std::max(1, P.max_packed) + 8ll * draw_stride + 16 + channel_count;
+        int64_t b = state_bytes + 64ll * std::max(1, P.max_packed) + 8ll * draw_stride + 24 + channel_count;
         b += 8ll * histogram_ctas(n) * P.max_bins;
         if (tiles) b += 8ll * (tp.rows_per_state + 1) * tp.columns;
         return b;
@@ -273,6 +349,7 @@ extern "C" int32_t qm_trajectories_run(qm_context* ctx, int32_t qubits, int32_t 
     double *table = nullptr, *partials = nullptr, *d_draws = nullptr, *tpart = nullptr, *tout = nullptr;
     double *d_masses = nullptr, *mean = nullptr, *m2 = nullptr;
     int32_t *counters = nullptr, *status = nullptr, *ambiguous = nullptr;
+    uint32_t *frame_x = nullptr, *frame_z = nullptr;
     int8_t* d_branches = nullptr;
     Decision* d_decisions = nullptr;
     const uint64_t table_stride = 8ull * (uint64_t)std::max(1, P.max_packed);
@@ -282,6 +359,7 @@ extern "C" int32_t qm_trajectories_run(qm_context* ctx, int32_t qubits, int32_t 
         (rc = buf.get(d_draws, sizeof(double) * (size_t)B * draw_stride)) ||
         (rc = buf.get(counters, sizeof(int32_t) * (size_t)B)) || (rc = buf.get(status, sizeof(int32_t) * (size_t)B)) ||
         (rc = buf.get(ambiguous, sizeof(int32_t) * (size_t)B)) ||
+        (rc = buf.get(frame_x, sizeof(uint32_t) * (size_t)B)) || (rc = buf.get(frame_z, sizeof(uint32_t) * (size_t)B)) ||
         (rc = buf.get(d_decisions, sizeof(Decision) * P.all_decisions.size())))
         return rc;
     if (out.branches && channel_count > 0 && (rc = buf.get(d_branches, (size_t)B * channel_count))) return rc;
@@ -306,6 +384,7 @@ extern "C" int32_t qm_trajectories_run(qm_context* ctx, int32_t qubits, int32_t 
     const double margin = precision == QM_FP32 ? 1e-5 : 1e-12;
     std::vector<double> h_out;
     std::vector<int32_t> h_counters((size_t)B), h_status((size_t)B), h_amb((size_t)B);
+    std::vector<uint32_t> h_fx((size_t)B), h_fz((size_t)B);
     std::vector<int8_t> h_branches;
     float device_ms = 0;
     int32_t waves = 0;
@@ -317,6 +396,8 @@ extern "C" int32_t qm_trajectories_run(qm_context* ctx, int32_t qubits, int32_t 
         QM_CUDA(cudaMemsetAsync(counters, 0, sizeof(int32_t) * Bw, st));
         QM_CUDA(cudaMemsetAsync(status, 0, sizeof(int32_t) * Bw, st));
         QM_CUDA(cudaMemsetAsync(ambiguous, 0, sizeof(int32_t) * Bw, st));
+        QM_CUDA(cudaMemsetAsync(frame_x, 0, sizeof(uint32_t) * Bw, st));
+        QM_CUDA(cudaMemsetAsync(frame_z, 0, sizeof(uint32_t) * Bw, st));
         if (d_branches) QM_CUDA(cudaMemsetAsync(d_branches, 0xff, (size_t)Bw * channel_count, st));
         if (draw_stride > 0)
             QM_CUDA(cudaMemcpyAsync(d_draws, draws + t0 * draw_stride, sizeof(double) * (size_t)Bw * draw_stride,
@@ -339,6 +420,8 @@ extern "C" int32_t qm_trajectories_run(qm_context* ctx, int32_t qubits, int32_t 
             da.branches = d_branches;
             da.channels = channel_count;
             da.margin = margin;
+            da.frame_x = frame_x;
+            da.frame_z = frame_z;
             QM_CUDA(launch_decide(da, Bw, st));
             for (size_t p = 0; p < s.plan.passes.size(); ++p) {
                 FusedBatch fb{Bw, 1ull << n, table, table_stride, s.pass_first[p], s.pass_count[p]};
@@ -357,6 +440,8 @@ extern "C" int32_t qm_trajectories_run(qm_context* ctx, int32_t qubits, int32_t 
         QM_CUDA(cudaMemcpyAsync(h_counters.data(), counters, sizeof(int32_t) * Bw, cudaMemcpyDeviceToHost, st));
         QM_CUDA(cudaMemcpyAsync(h_status.data(), status, sizeof(int32_t) * Bw, cudaMemcpyDeviceToHost, st));
         QM_CUDA(cudaMemcpyAsync(h_amb.data(), ambiguous, sizeof(int32_t) * Bw, cudaMemcpyDeviceToHost, st));
+        QM_CUDA(cudaMemcpyAsync(h_fx.data(), frame_x, sizeof(uint32_t) * Bw, cudaMemcpyDeviceToHost, st));
+        QM_CUDA(cudaMemcpyAsync(h_fz.data(), frame_z, sizeof(uint32_t) * Bw, cudaMemcpyDeviceToHost, st));
         if (d_branches) {
             h_branches.resize((size_t)Bw * channel_count);
             QM_CUDA(cudaMemcpyAsync(h_branches.data(), d_branches, h_branches.size(), cudaMemcpyDeviceToHost, st));
@@ -372,6 +457,10 @@ extern "C" int32_t qm_trajectories_run(qm_context* ctx, int32_t qubits, int32_t 
                 return fail(QM_E_MASS, "trajectory " + std::to_string(t0 + b) +
                                            ": The state has no finite positive probability mass.");
         }
+        if (out.outcomes) {  // the true state: the frame's X applied to the stored one
+            QM_CUDA(launch_frame_flip(amps, n, precision, Bw, frame_x, st));
+            QM_CUDA(cudaStreamSynchronize(st));
+        }
         for (int b = 0; b < Bw; ++b) {
             const int64_t t = t0 + b;
             int32_t consumed = h_counters[(size_t)b];
@@ -383,7 +472,10 @@ extern "C" int32_t qm_trajectories_run(qm_context* ctx, int32_t qubits, int32_t 
                 for (int32_t k = 0; k < term_count && out.values; ++k) {
                     const double raw = h_out[(size_t)b * tp.columns + k];
                     if (!std::isfinite(raw)) return fail(QM_E_MASS, "The observable accumulation is nonfinite.");
-                    out.values[t * term_count + k] = raw / mass;
+                    // <F psi|P|F psi> = -<psi|P|psi> when the frame anticommutes with P
+                    const int odd = (__builtin_popcount(h_fx[(size_t)b] & terms[k].sign_mask) +
+                                     __builtin_popcount(h_fz[(size_t)b] & terms[k].flip_mask)) & 1;
+                    out.values[t * term_count + k] = odd ? -(raw / mass) : raw / mass;
                 }
             }
             if (out.ambiguous) out.ambiguous[t] = h_amb[(size_t)b];
@@ -412,7 +504,9 @@ extern "C" int32_t qm_trajectories_run(qm_context* ctx, int32_t qubits, int32_t 
             std::vector<double> hm((size_t)Bw);
             for (int b = 0; b < Bw; ++b) hm[(size_t)b] = h_out[(size_t)b * tp.columns + tp.mass_column];
             QM_CUDA(cudaMemcpyAsync(d_masses, hm.data(), sizeof(double) * Bw, cudaMemcpyHostToDevice, st));
-            QM_CUDA(launch_welford(amps, precision, Bw, 1ull << n, len, d_masses, t0, mean, m2, st));
+            // after a frame flip (outcomes) the stored states are the true ones
+            if (out.outcomes) QM_CUDA(cudaMemsetAsync(frame_x, 0, sizeof(uint32_t) * Bw, st));
+            QM_CUDA(launch_welford(amps, precision, Bw, 1ull << n, len, d_masses, frame_x, t0, mean, m2, st));
             QM_CUDA(cudaStreamSynchronize(st));
         }
     }
