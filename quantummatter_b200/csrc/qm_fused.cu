@@ -84,17 +84,39 @@ struct Layout {
     }
 };
 
+// Registers whose index has bit m set, as a 2^R-bit pattern.
+__host__ __device__ constexpr uint32_t reg_half(int m) {
+    uint32_t p = 0;
+    for (int i = 0; i < NR; ++i)
+        if ((i >> m) & 1) p |= 1u << i;
+    return p;
+}
+
+// Bit i is set when register i has every local bit of cm set: the thread bits of cm must all
+// be set in this thread's base index, and each register bit of cm keeps half the registers.
+__device__ __forceinline__ uint32_t control_pattern(const Layout& L, uint32_t cm) {
+    uint32_t regs = 0, pat = (NR == 32) ? 0xffffffffu : ((1u << NR) - 1u);
+#pragma unroll
+    for (int m = 0; m < R; ++m)
+        if (cm & L.pm[m]) {
+            regs |= L.pm[m];
+            pat &= reg_half(m);
+        }
+    const uint32_t thread_bits = cm & ~regs;
+    return (L.base & thread_bits) == thread_bits ? pat : 0u;
+}
+
 template <typename T, int M, bool REAL, bool CTRL>
 __device__ __forceinline__ void op_matrix(Cx<T> (&a)[NR], const FusedOp& op, const Coef& c, const Layout& L) {
     const T ar = (T)c.v[0], br = (T)c.v[2], cr = (T)c.v[4], dr = (T)c.v[6];
     const T ai = REAL ? (T)0 : (T)c.v[1], bi = REAL ? (T)0 : (T)c.v[3];
     const T ci = REAL ? (T)0 : (T)c.v[5], di = REAL ? (T)0 : (T)c.v[7];
-    const uint32_t cm = op.cmask_local;
+    const uint32_t pat = CTRL ? control_pattern(L, op.cmask_local) : 0u;
 #pragma unroll
     for (int i = 0; i < NR; ++i) {
         if ((i >> M) & 1) continue;
         const int k = i | (1 << M);
-        if (CTRL && (L.local(i) & cm) != cm) continue;
+        if (CTRL && !((pat >> i) & 1u)) continue;
         Cx<T> x = a[i], y = a[k];
         if (REAL) {
             a[i] = Cx<T>{ar * x.re + br * y.re, ar * x.im + br * y.im};
@@ -162,12 +184,12 @@ __device__ __forceinline__ void op_branch(Cx<T> (&a)[NR], const FusedOp& op, con
 // a per-amplitude predicate.
 template <typename T, int M>
 __device__ __forceinline__ void op_exchange(Cx<T> (&a)[NR], const FusedOp& op, const Layout& L) {
-    const uint32_t cm = op.cmask_local;
+    const uint32_t pat = control_pattern(L, op.cmask_local);
 #pragma unroll
     for (int i = 0; i < NR; ++i) {
         if ((i >> M) & 1) continue;
         const int k = i | (1 << M);
-        const bool on = (L.local(i) & cm) == cm;
+        const bool on = (pat >> i) & 1u;
         Cx<T> x = a[i], y = a[k];
         a[i] = on ? y : x;
         a[k] = on ? x : y;
@@ -179,6 +201,7 @@ __device__ __forceinline__ void op_exchange(Cx<T> (&a)[NR], const FusedOp& op, c
 template <typename T, int M, int MC>
 __device__ __forceinline__ void op_exchange_rc(Cx<T> (&a)[NR], const FusedOp& op, const Layout& L) {
     const uint32_t cm = op.cmask_local & ~L.pm[MC];
+    const uint32_t pat = cm ? control_pattern(L, cm) : 0u;
 #pragma unroll
     for (int i = 0; i < NR; ++i) {
         if (((i >> M) & 1) || !((i >> MC) & 1)) continue;
@@ -188,7 +211,7 @@ __device__ __forceinline__ void op_exchange_rc(Cx<T> (&a)[NR], const FusedOp& op
             a[i] = y;
             a[k] = x;
         } else {
-            const bool on = (L.local(i) & cm) == cm;
+            const bool on = (pat >> i) & 1u;
             a[i] = on ? y : x;
             a[k] = on ? x : y;
         }
@@ -222,12 +245,12 @@ __device__ __forceinline__ void op_exchange_any(Cx<T> (&a)[NR], const FusedOp& o
 // SWAP of register bits M1 and M2: exchanges the (M1=1, M2=0) and (M1=0, M2=1) members.
 template <typename T, int M1, int M2>
 __device__ __forceinline__ void op_swap(Cx<T> (&a)[NR], const FusedOp& op, const Layout& L) {
-    const uint32_t cm = op.cmask_local;
+    const uint32_t pat = control_pattern(L, op.cmask_local);
 #pragma unroll
     for (int i = 0; i < NR; ++i) {
         if (!((i >> M1) & 1) || ((i >> M2) & 1)) continue;
         const int k = i ^ (1 << M1) ^ (1 << M2);
-        const bool on = (L.local(i) & cm) == cm;
+        const bool on = (pat >> i) & 1u;
         Cx<T> x = a[i], y = a[k];
         a[i] = on ? y : x;
         a[k] = on ? x : y;
@@ -268,10 +291,10 @@ template <typename T, int M>
 __device__ __forceinline__ void op_diag_reg(Cx<T> (&a)[NR], const FusedOp& op, const Coef& c, const Layout& L) {
     const T ar = (T)c.v[0], ai = (T)c.v[1], dr = (T)c.v[6], di = (T)c.v[7];
     const bool a_one = op.flags & 1, d_one = op.flags & 2;
-    const uint32_t cm = op.cmask_local;
+    const uint32_t pat = control_pattern(L, op.cmask_local);
 #pragma unroll
     for (int i = 0; i < NR; ++i) {
-        if (cm != 0 && (L.local(i) & cm) != cm) continue;
+        if (!((pat >> i) & 1u)) continue;
         if ((i >> M) & 1) {
             if (!d_one) a[i] = cmul<T>(dr, di, a[i]);
         } else if (!a_one) {
@@ -312,19 +335,20 @@ __device__ __forceinline__ void op_diag(Cx<T> (&a)[NR], const FusedOp& op, const
     }
     if (bit ? d_one : a_one) return;
     const T pr = bit ? dr : ar, pi = bit ? di : ai;
+    const uint32_t pat = control_pattern(L, cm);
 #pragma unroll
     for (int i = 0; i < NR; ++i) {
-        if (cm != 0 && (L.local(i) & cm) != cm) continue;
+        if (!((pat >> i) & 1u)) continue;
         a[i] = cmul<T>(pr, pi, a[i]);
     }
 }
 
 template <typename T>
 __device__ __forceinline__ void op_negate(Cx<T> (&a)[NR], const FusedOp& op, const Layout& L) {
-    const uint32_t cm = op.cmask_local;
+    const uint32_t pat = control_pattern(L, op.cmask_local);
 #pragma unroll
     for (int i = 0; i < NR; ++i) {
-        const bool on = (L.local(i) & cm) == cm;
+        const bool on = (pat >> i) & 1u;
         a[i].re = on ? -a[i].re : a[i].re;
         a[i].im = on ? -a[i].im : a[i].im;
     }
@@ -352,6 +376,7 @@ __device__ __forceinline__ void op_diag_group(Cx<T> (&a)[NR], const FusedOp* mem
         on[m] = Cx<T>{(T)1, (T)0};
     }
     uint32_t negate = 0;  // bit i: register i changes sign
+    bool phased = false;  // some member is more than a sign
     uint32_t regmask = 0;
 #pragma unroll
     for (int m = 0; m < R; ++m) regmask |= L.pm[m];
@@ -359,19 +384,10 @@ __device__ __forceinline__ void op_diag_group(Cx<T> (&a)[NR], const FusedOp* mem
         const FusedOp& op = members[k];
         if ((outer & op.cmask_outer) != op.cmask_outer) continue;
         if (op.code == OP_NEGATE) {
-            const uint32_t cm = op.cmask_local;
-            if ((L.base & cm & ~regmask) != (cm & ~regmask)) continue;  // a thread-bit factor is zero
-            uint32_t rm = 0;                                             // register indices in the mask
-#pragma unroll
-            for (int m = 0; m < R; ++m)
-                if (cm & L.pm[m]) rm |= 1u << m;
-            uint32_t pattern = 0;
-#pragma unroll
-            for (int i = 0; i < NR; ++i)
-                if ((i & rm) == rm) pattern |= 1u << i;
-            negate ^= pattern;
+            negate ^= control_pattern(L, op.cmask_local);
             continue;
         }
+        phased = true;
         // uncontrolled single-qubit diagonal
         const double* src = (op.flags & kOpTable) ? table + 8 * (size_t)op.reserved : op.coef;
         const Cx<T> pa{(T)src[0], (T)src[1]}, pd{(T)src[6], (T)src[7]};
@@ -387,6 +403,15 @@ __device__ __forceinline__ void op_diag_group(Cx<T> (&a)[NR], const FusedOp* mem
         }
         const bool bit = lt < 0 ? (outer & op.target_outer) != 0 : ((L.base >> lt) & 1u) != 0;
         u = cmulc<T>(u, bit ? pd : pa);
+    }
+    if (!phased) {  // only CZ / Z members: signs
+#pragma unroll
+        for (int i = 0; i < NR; ++i) {
+            const bool neg = (negate >> i) & 1u;
+            a[i].re = neg ? -a[i].re : a[i].re;
+            a[i].im = neg ? -a[i].im : a[i].im;
+        }
+        return;
     }
     // phase[i] = lo[i & low] * hi[i >> LB]: two small product tables instead of a full tree,
     // to keep the live registers low
@@ -524,8 +549,23 @@ __global__ void __launch_bounds__(1 << (K - R), ((sizeof(T) == 8 && K == 12) || 
             Coef c;
             if (code == OP_MATRIX || code == OP_MATRIX_REAL || code == OP_DIAG) {
                 const double* src = (op.flags & kOpTable) ? table + 8 * (size_t)op.reserved : op.coef;
+                // only the entries the op kind reads
+                if (code == OP_MATRIX) {
 #pragma unroll
-                for (int k = 0; k < 8; ++k) c.v[k] = src[k];
+                    for (int k = 0; k < 8; ++k) c.v[k] = src[k];
+                } else if (code == OP_MATRIX_REAL) {
+#pragma unroll
+                    for (int k = 0; k < 8; k += 2) {
+                        c.v[k] = src[k];
+                        c.v[k + 1] = 0.0;
+                    }
+                } else {
+                    c.v[0] = src[0];
+                    c.v[1] = src[1];
+                    c.v[6] = src[6];
+                    c.v[7] = src[7];
+                    c.v[2] = c.v[3] = c.v[4] = c.v[5] = 0.0;
+                }
             }
             switch (code) {
             case OP_MATRIX:
