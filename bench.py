@@ -336,6 +336,129 @@ def run_trajectories(args) -> None:
     ctx.Dispose()
 
 
+def serving_requests(count: int, rate: float, precision: int, seed: int, sessions):
+    """Poisson arrivals at `rate`; each request an expectation of a random brick circuit (Z_i and
+    Z_i Z_i+1), 1000 shots of one, or a VQE step of a random session (TFIM chain, hardware-efficient
+    ansatz of 2 layers); qubits uniform in [10, 28], brick depth uniform in [10, 100]."""
+    import numpy as np
+
+    from quantummatter_b200.observables import PauliString
+    from quantummatter_b200.serving import ExpectationRequest, ShotsRequest, VqeStepRequest
+    from quantummatter_b200.workloads import brick_circuit
+    rng = np.random.default_rng(seed)
+    t, arrivals, reqs = 0.0, [], []
+    for i in range(count):
+        t += rng.exponential(1.0 / rate)
+        arrivals.append(t)
+        kind = int(rng.integers(3))
+        if kind == 2:
+            reqs.append(VqeStepRequest(sessions[int(rng.integers(len(sessions)))]))
+            continue
+        n, depth = int(rng.integers(10, 29)), int(rng.integers(10, 101))
+        c = brick_circuit(n, depth, seed=seed * 1000 + i)
+        if kind == 0:
+            obs = [PauliString("".join("Z" if q == j else "I" for q in reversed(range(n)))) for j in range(n)]
+            obs += [PauliString("".join("Z" if q in (j, j + 1) else "I" for q in reversed(range(n)))) for j in range(n - 1)]
+            reqs.append(ExpectationRequest(c, obs, precision))
+        else:
+            reqs.append(ShotsRequest(c, shots=1000, seed=i, precision=precision))
+    return reqs, arrivals
+
+
+def serving_sessions(count: int, precision: int, seed: int):
+    import numpy as np
+
+    from quantummatter_b200.serving import VqeSession
+    from quantummatter_b200.workloads import hardware_efficient_ansatz, tfim_chain
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = int(rng.integers(10, 29))
+        c = hardware_efficient_ansatz(n, 2)
+        out.append(VqeSession(c, tfim_chain(n, seed=seed + i), rng.uniform(-np.pi, np.pi, c.ParameterCount),
+                              step_size=0.05, precision=precision))
+    return out
+
+
+def serving_summary(responses, reqs, makespan: float) -> dict:
+    import numpy as np
+
+    from quantummatter_b200.serving import VqeStepRequest
+    lat = np.array([r.latency for r in responses])
+    evals = sum(1 + 2 * len(q.session.circuit.RotationParameterIndices) for q in reqs if isinstance(q, VqeStepRequest))
+    per_kind = {}
+    for kind in ("expectation", "shots", "vqe_step"):
+        k = np.array([r.latency for r in responses if r.kind == kind])
+        if k.size:
+            per_kind[kind] = {"count": int(k.size), "p50_ms": float(np.percentile(k, 50) * 1e3),
+                              "p99_ms": float(np.percentile(k, 99) * 1e3)}
+    return {"requests": len(responses), "makespan_s": makespan, "requests_per_s": len(responses) / makespan,
+            "energy_evals_per_s": evals / makespan, "energy_evals": evals,
+            "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
+            "mean_vqe_batch": float(np.mean([r.batch for r in responses if r.kind == "vqe_step"] or [1])),
+            "per_kind": per_kind}
+
+
+def run_serving(args) -> None:
+    """Serving: Poisson request streams at swept rates through the batching server (FP32 and FP64),
+    and the plain form (one request at a time, FP64, unbatched) on the same stream."""
+    from quantummatter_b200.backend import FP32, FP64, B200BackendOptions, B200Context
+    from quantummatter_b200.serving import B200Server, serve_plain
+    rates = [float(r) for r in args.rates.split(",")]
+    results = {}
+    clocks = ClockSampler(0)
+    with clocks:
+        for name, prec in (("fp32", FP32), ("fp64", FP64)):
+            for rate in rates:
+                sessions = serving_sessions(args.sessions, prec, seed=7)
+                reqs, arrivals = serving_requests(args.requests, rate, prec, seed=11, sessions=sessions)
+                with B200Server(workers=args.workers, budget_bytes=args.serve_budget << 30,
+                                context_budget_bytes=24 << 30, cache_bytes=8 << 30) as server:
+                    # warm-up: kernel attributes and plans of each kind
+                    warm = serving_sessions(1, prec, seed=3)
+                    wr, _ = serving_requests(3, 1.0, prec, seed=5, sessions=warm)
+                    for f in [server.submit(r) for r in wr]:
+                        f.result()
+                    t0 = time.perf_counter()
+                    futures = []
+                    for req, at in zip(reqs, arrivals):
+                        wait = t0 + at - time.perf_counter()
+                        if wait > 0:
+                            time.sleep(wait)
+                        futures.append(server.submit(req))
+                    responses = [f.result() for f in futures]
+                    makespan = max(r.finished for r in responses) - t0
+                results[f"{name}_rate{rate:g}"] = serving_summary(responses, reqs, makespan)
+        # plain form at the lowest rate on the same stream (FP64)
+        ctx = B200Context(B200BackendOptions(DeviceMemoryBudgetBytes=24 << 30, StagingMemoryBudgetBytes=1 << 30))
+        sessions = serving_sessions(args.sessions, FP64, seed=7)
+        reqs, arrivals = serving_requests(args.requests, rates[0], FP64, seed=11, sessions=sessions)
+        warm = serving_sessions(1, FP64, seed=3)
+        serve_plain(serving_requests(3, 1.0, FP64, seed=5, sessions=warm)[0], ctx)
+        t0 = time.perf_counter()
+        plain = serve_plain(reqs, ctx, arrivals)
+        results[f"plain_fp64_rate{rates[0]:g}"] = serving_summary(plain, reqs, max(r.finished for r in plain) - t0)
+        ctx.Dispose()
+    top = results[f"fp32_rate{rates[-1]:g}"]
+    same = results[f"fp64_rate{rates[0]:g}"]
+    plain = results[f"plain_fp64_rate{rates[0]:g}"]
+    line = {
+        "metric": "served energy evals/s", "value": top["energy_evals_per_s"], "unit": "evals/s", "n_gpus": 1,
+        "higher_is_better": True, "dtype": "f32", "data": "synthetic", "scaling": "weak", "vs_baseline": None,
+        "config": {"workload": "Poisson request stream: expectations of random brick circuits (depth 10-100), 1000 "
+                               "shots, or VQE steps (TFIM chains, 2-layer hardware-efficient ansatz); qubits 10-28; "
+                               f"admission budget {args.serve_budget} GiB at 16 * 2^n (FP64) or 8 * 2^n (FP32) bytes "
+                               f"per request; {args.workers} workers; {args.requests} requests per rate",
+                   "rates_per_s": rates, "sessions": args.sessions},
+        "p99_ms": top["p99_ms"], "p50_ms": top["p50_ms"],
+        f"fp64_p99_ms_rate{rates[0]:g}": same["p99_ms"], f"plain_fp64_p99_ms_rate{rates[0]:g}": plain["p99_ms"],
+        "p99_vs_plain_fp64": same["p99_ms"] / plain["p99_ms"],
+        "energy_evals_per_s_vs_plain_fp64": same["energy_evals_per_s"] / plain["energy_evals_per_s"],
+        "results": results, "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -348,13 +471,18 @@ def main() -> None:
     ap.add_argument("--depth", type=int, default=DEPTH)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="brick", choices=["brick", "vqe", "trajectories"])
+    ap.add_argument("--workload", default="brick", choices=["brick", "vqe", "trajectories", "serving"])
     ap.add_argument("--sizes", default="16,18,20,22", help="vqe workload: qubit counts")
     ap.add_argument("--vectors", type=int, default=128, help="vqe workload: parameter vectors per size")
     ap.add_argument("--traj-qubits", type=int, default=24, help="trajectories workload: qubits")
     ap.add_argument("--traj-depth", type=int, default=30, help="trajectories workload: layers")
     ap.add_argument("--trajectories", type=int, default=1024, help="trajectories workload: trajectories")
     ap.add_argument("--traj-precision", default="fp32", choices=["fp64", "fp32"])
+    ap.add_argument("--rates", default="1,3", help="serving workload: arrival rates per second")
+    ap.add_argument("--requests", type=int, default=40, help="serving workload: requests per rate")
+    ap.add_argument("--sessions", type=int, default=12, help="serving workload: VQE sessions")
+    ap.add_argument("--workers", type=int, default=4, help="serving workload: worker streams")
+    ap.add_argument("--serve-budget", type=int, default=96, help="serving workload: admission budget, GiB")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -364,6 +492,9 @@ def main() -> None:
         return
     if args.workload == "trajectories":
         run_trajectories(args)
+        return
+    if args.workload == "serving":
+        run_serving(args)
         return
 
     dist, rank, world, local = dist_setup(args.gpus)

@@ -332,6 +332,14 @@ int32_t qm_vqe_evaluate(qm_context* context, int32_t qubits, int32_t precision, 
                         int32_t operation_count, int32_t parameter_count, const qm_pauli_term* terms,
                         int32_t term_count, const double* parameters, int32_t vectors, int32_t with_gradient,
                         double* energies, double* gradients, qm_vqe_stats* stats);
+/* qm_vqe_evaluate with its own Hamiltonian coefficients per vector: coefficients[vector][term]
+ * replaces terms[t].coefficient, so vectors whose Hamiltonians share Pauli strings but not
+ * coefficients (served requests on different chains) share one batch. */
+int32_t qm_vqe_evaluate_coefficients(qm_context* context, int32_t qubits, int32_t precision,
+                                     const qm_template_op* operations, int32_t operation_count, int32_t parameter_count,
+                                     const qm_pauli_term* terms, int32_t term_count, const double* coefficients,
+                                     const double* parameters, int32_t vectors, int32_t with_gradient,
+                                     double* energies, double* gradients, qm_vqe_stats* stats);
 
 /* ---------------------------------------------------------------- noise trajectories */
 

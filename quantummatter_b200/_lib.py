@@ -147,6 +147,8 @@ SIGNATURES = {
     "qm_batch_expectation": (I32, [P, I32, C.POINTER(PauliTermC), I32, DP, DP]),
     "qm_vqe_evaluate": (I32, [P, I32, I32, C.POINTER(TemplateOp), I32, I32, C.POINTER(PauliTermC), I32, DP, I32, I32,
                               DP, DP, C.POINTER(VqeStats)]),
+    "qm_vqe_evaluate_coefficients": (I32, [P, I32, I32, C.POINTER(TemplateOp), I32, I32, C.POINTER(PauliTermC), I32,
+                                           DP, DP, I32, I32, DP, DP, C.POINTER(VqeStats)]),
     "qm_trajectories_run": (I32, [P, I32, I32, C.POINTER(Gate), I32, C.POINTER(ChannelC), I32, I32, DP, I32,
                                   C.POINTER(PauliTermC), I32, C.POINTER(TrajectoryOutputs),
                                   C.POINTER(TrajectoryStats)]),

@@ -399,10 +399,13 @@ void neumaier_add(double& sum, double& correction, double value) {
 
 }  // namespace
 
-extern "C" int32_t qm_vqe_evaluate(qm_context* ctx, int32_t qubits, int32_t precision, const qm_template_op* ops,
-                                   int32_t op_count, int32_t parameter_count, const qm_pauli_term* terms,
-                                   int32_t term_count, const double* parameters, int32_t vectors, int32_t with_gradient,
-                                   double* energies, double* gradients, qm_vqe_stats* stats) {
+namespace {
+
+// coefficients: [vectors][term_count] per-vector term coefficients, or null for the terms' own.
+int32_t vqe_evaluate(qm_context* ctx, int32_t qubits, int32_t precision, const qm_template_op* ops, int32_t op_count,
+                     int32_t parameter_count, const qm_pauli_term* terms, int32_t term_count, const double* coefficients,
+                     const double* parameters, int32_t vectors, int32_t with_gradient, double* energies,
+                     double* gradients, qm_vqe_stats* stats) {
     auto wall0 = std::chrono::steady_clock::now();
     if (!ctx) return fail(QM_E_ARG, "context is null");
     if (qubits < 1 || qubits > 30) return fail(QM_E_RANGE, "qubits must be between 1 and 30");
@@ -417,8 +420,14 @@ extern "C" int32_t qm_vqe_evaluate(qm_context* ctx, int32_t qubits, int32_t prec
     const uint32_t all = (uint32_t)((1ull << qubits) - 1);
     for (int32_t t = 0; t < term_count; ++t) {
         if ((terms[t].flip_mask | terms[t].sign_mask) & ~all) return fail(QM_E_ARG, "Circuit and Hamiltonian sizes must match.");
-        if (!std::isfinite(terms[t].coefficient)) return fail(QM_E_RANGE, "coefficient must be finite");
+        if (!coefficients && !std::isfinite(terms[t].coefficient)) return fail(QM_E_RANGE, "coefficient must be finite");
     }
+    if (coefficients)
+        for (int64_t i = 0; i < (int64_t)vectors * term_count; ++i)
+            if (!std::isfinite(coefficients[i])) return fail(QM_E_RANGE, "coefficient must be finite");
+    auto coef = [&](int v, int t) {
+        return coefficients ? coefficients[(size_t)v * term_count + t] : terms[t].coefficient;
+    };
     for (int64_t i = 0; i < (int64_t)vectors * parameter_count; ++i)
         if (!std::isfinite(parameters[i])) return fail(QM_E_RANGE, "Parameters must be finite.");
 
@@ -654,10 +663,11 @@ extern "C" int32_t qm_vqe_evaluate(qm_context* ctx, int32_t qubits, int32_t prec
         }
         double sum = 0, corr = 0;
         for (int t = 0; t < term_count; ++t) {
-            if (terms[t].coefficient == 0) continue;
+            const double ct = coef(v, t);
+            if (ct == 0) continue;
             double e;
             if (!value(c0, t, e)) return fail(QM_E_MASS, "The observable accumulation is nonfinite.");
-            neumaier_add(sum, corr, terms[t].coefficient * e);
+            neumaier_add(sum, corr, ct * e);
             if (!std::isfinite(sum) || !std::isfinite(corr)) return fail(QM_E_MASS, "The energy accumulation is nonfinite.");
         }
         const double energy = sum + corr;
@@ -677,7 +687,7 @@ extern "C" int32_t qm_vqe_evaluate(qm_context* ctx, int32_t qubits, int32_t prec
             for (int t = 0; t < term_count; ++t) {
                 double plus, minus;
                 if (!value(cp, t, plus) || !value(cm, t, minus)) return fail(QM_E_MASS, "The observable accumulation is nonfinite.");
-                const double contribution = terms[t].coefficient * (0.5 * plus - 0.5 * minus);
+                const double contribution = coef(v, t) * (0.5 * plus - 0.5 * minus);
                 neumaier_add(grad[p], correction[(size_t)p], contribution);
                 if (!std::isfinite(grad[p]) || !std::isfinite(correction[(size_t)p]))
                     return fail(QM_E_MASS, "The gradient accumulation is nonfinite.");
@@ -699,4 +709,25 @@ extern "C" int32_t qm_vqe_evaluate(qm_context* ctx, int32_t qubits, int32_t prec
         stats->wall_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - wall0).count();
     }
     return QM_OK;
+}
+
+}  // namespace
+
+extern "C" int32_t qm_vqe_evaluate(qm_context* ctx, int32_t qubits, int32_t precision, const qm_template_op* ops,
+                                   int32_t op_count, int32_t parameter_count, const qm_pauli_term* terms,
+                                   int32_t term_count, const double* parameters, int32_t vectors, int32_t with_gradient,
+                                   double* energies, double* gradients, qm_vqe_stats* stats) {
+    return vqe_evaluate(ctx, qubits, precision, ops, op_count, parameter_count, terms, term_count, nullptr, parameters,
+                        vectors, with_gradient, energies, gradients, stats);
+}
+
+extern "C" int32_t qm_vqe_evaluate_coefficients(qm_context* ctx, int32_t qubits, int32_t precision,
+                                                const qm_template_op* ops, int32_t op_count, int32_t parameter_count,
+                                                const qm_pauli_term* terms, int32_t term_count,
+                                                const double* coefficients, const double* parameters, int32_t vectors,
+                                                int32_t with_gradient, double* energies, double* gradients,
+                                                qm_vqe_stats* stats) {
+    if (term_count > 0 && !coefficients) return fail(QM_E_ARG, "coefficients is null");
+    return vqe_evaluate(ctx, qubits, precision, ops, op_count, parameter_count, terms, term_count, coefficients,
+                        parameters, vectors, with_gradient, energies, gradients, stats);
 }

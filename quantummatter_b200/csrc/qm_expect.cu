@@ -163,13 +163,10 @@ cudaError_t launch_tile_k(const void* amps, int qubits, const TilePass& tp, cons
     L.partials = partials;
     for (int i = 0; i < tp.term_count; ++i) L.t[i] = terms[tp.term_begin + i];
     const size_t smem = (sizeof(V) << K) + sizeof(double) * (size_t)((1 << (K - R)) / 32) * (tp.term_count + 1);
-    static bool configured = false;
-    if (!configured) {
-        cudaError_t e = cudaFuncSetAttribute(k_expect_tile<T, K, MAXT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)((sizeof(V) << K) + sizeof(double) * ((1 << (K - R)) / 32) * (MAXT + 1)));
-        if (e != cudaSuccess) return e;
-        configured = true;
-    }
+    static const cudaError_t configured =  // once per process, thread-safe
+        cudaFuncSetAttribute(k_expect_tile<T, K, MAXT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)((sizeof(V) << K) + sizeof(double) * ((1 << (K - R)) / 32) * (MAXT + 1)));
+    if (configured != cudaSuccess) return configured;
     dim3 grid(1u << (qubits - K), (unsigned)states);
     k_expect_tile<T, K, MAXT><<<grid, 1 << (K - R), smem, st>>>(reinterpret_cast<const V*>(amps), L);
     return cudaGetLastError();

@@ -630,18 +630,24 @@ cudaError_t launch_k(void* amps, int qubits, const FusedPass& p, const FusedOp* 
     L.table_slots = !tabled ? 0 : batch->slot_count >= 0 ? batch->slot_count : (int32_t)(batch->table_stride / 8);
     L.pad = 0;
     const size_t smem = tile_bytes<T, K>() + program_bytes(p.op_count) + sizeof(double) * 8 * (size_t)L.table_slots;
-    static int optin = 0, sms = 0;
-    if (!optin) {
+    // device limits and the kernel's shared-memory opt-in, set once per process (thread-safe:
+    // several host threads may launch at the same time)
+    struct Limits {
+        cudaError_t err;
+        int optin, sms;
+    };
+    static const Limits lim = [] {
+        Limits l{cudaSuccess, 0, 0};
         int dev = 0;
-        cudaError_t e = cudaGetDevice(&dev);
-        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fused<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
-        if (e != cudaSuccess) {
-            optin = 0;
-            return e;
-        }
-    }
+        l.err = cudaGetDevice(&dev);
+        if (l.err == cudaSuccess) l.err = cudaDeviceGetAttribute(&l.optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+        if (l.err == cudaSuccess) l.err = cudaDeviceGetAttribute(&l.sms, cudaDevAttrMultiProcessorCount, dev);
+        if (l.err == cudaSuccess)
+            l.err = cudaFuncSetAttribute(k_fused<T, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, l.optin);
+        return l;
+    }();
+    if (lim.err != cudaSuccess) return lim.err;
+    const int optin = lim.optin, sms = lim.sms;
     if (smem > (size_t)optin) return cudaErrorInvalidValue;  // program or coefficient row too large
     int per_sm = 0;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fused<T, K>, 1 << (K - R), smem);

@@ -169,7 +169,10 @@ class B200VariationalEnergyEvaluator:
             raise ArgumentError("Circuit and Hamiltonian sizes must match.")
 
     def EvaluateBatch(self, circuit: ParameterizedCircuit, hamiltonian: PauliHamiltonian,
-                      parameters: np.ndarray, withGradient: bool = True) -> BatchEvaluation:
+                      parameters: np.ndarray, withGradient: bool = True,
+                      coefficients: np.ndarray | None = None) -> BatchEvaluation:
+        """Energies (and gradients) of every parameter vector.  `coefficients` ([vectors][terms])
+        replaces the Hamiltonian's own coefficients per vector (same Pauli strings)."""
         self._validate(circuit, hamiltonian)
         params = np.ascontiguousarray(parameters, dtype=np.float64)
         if params.ndim == 1:
@@ -182,9 +185,20 @@ class B200VariationalEnergyEvaluator:
         energies = np.zeros(vectors, dtype=np.float64)
         grads = np.zeros((vectors, max(1, pcount)), dtype=np.float64)
         stats = _lib.VqeStats()
-        check(load().qm_vqe_evaluate(self.context.handle, circuit.QubitCount, self.precision, ops, nops, pcount, terms,
-                                     nterms, params.ctypes.data_as(_lib.DP), vectors, 1 if withGradient else 0,
-                                     energies.ctypes.data_as(_lib.DP), grads.ctypes.data_as(_lib.DP), C.byref(stats)))
+        if coefficients is None:
+            check(load().qm_vqe_evaluate(self.context.handle, circuit.QubitCount, self.precision, ops, nops, pcount,
+                                         terms, nterms, params.ctypes.data_as(_lib.DP), vectors,
+                                         1 if withGradient else 0, energies.ctypes.data_as(_lib.DP),
+                                         grads.ctypes.data_as(_lib.DP), C.byref(stats)))
+        else:
+            coef = np.ascontiguousarray(coefficients, dtype=np.float64)
+            if coef.shape != (vectors, nterms):
+                raise ArgumentError("coefficients must be a [vectors][terms] array")
+            check(load().qm_vqe_evaluate_coefficients(self.context.handle, circuit.QubitCount, self.precision, ops,
+                                                      nops, pcount, terms, nterms, coef.ctypes.data_as(_lib.DP),
+                                                      params.ctypes.data_as(_lib.DP), vectors,
+                                                      1 if withGradient else 0, energies.ctypes.data_as(_lib.DP),
+                                                      grads.ctypes.data_as(_lib.DP), C.byref(stats)))
         return BatchEvaluation(energies, grads[:, :pcount] if withGradient else None, stats.circuits, stats.waves,
                                stats.batch_states, stats.passes_per_circuit, stats.tile_passes, stats.device_seconds,
                                stats.wall_seconds)
