@@ -279,16 +279,27 @@ def run_trajectories(args) -> None:
     D = nc.MaxDraws()
     obs = [PauliString("".join("Z" if q == i else "I" for q in reversed(range(n)))) for i in range(n)]
     obs += [PauliString("".join("Z" if q in (i, i + 1) else "I" for q in reversed(range(n)))) for i in range(n - 1)]
-    stream = random_doubles(DEFAULT_DRAW_SEED, T * D)
+    # ranks: each GPU runs its own T trajectories, the next slice of one seeded stream (weak
+    # scaling); the timed region is bracketed by barriers and timed as the max over ranks
+    dist, rank, world, local = dist_setup(args.gpus)
+    stream = random_doubles(DEFAULT_DRAW_SEED, T * D, skip=rank * T * D)
     rows = stream.reshape(T, D)
-    ctx = B200Context(B200BackendOptions(DeviceMemoryBudgetBytes=160 << 30, StagingMemoryBudgetBytes=1 << 30))
+    ctx = B200Context(B200BackendOptions(DeviceIndex=local, DeviceMemoryBudgetBytes=160 << 30,
+                                         StagingMemoryBudgetBytes=1 << 30))
     sim = B200NoisySimulator(ctx, precision=prec)
     sim.RunBatch(nc, rows[:8], obs)  # warm-up: plans, kernel attributes
-    clocks = ClockSampler(0)
+    clocks = ClockSampler(local)
+    barrier_max(dist, 0.0, local)
     with clocks:
         t0 = time.perf_counter()
         res = sim.RunBatch(nc, rows, obs)
         wall = time.perf_counter() - t0
+    wall = barrier_max(dist, wall, local)
+    if rank != 0:
+        ctx.Dispose()
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     # every trajectory drew once per placement, so the rows were the reference's draw order
     in_order = bool(np.all(res.consumed == D))
     dev = res.stats["device_seconds"]
@@ -314,7 +325,8 @@ def run_trajectories(args) -> None:
                "sample": f"oracle NoisyCircuit.Execute restatement, first of {depth} layers of one {n}-qubit "
                          f"trajectory ({time.perf_counter() - t1:.2f} s), scaled to the full depth"}
     line = {
-        "metric": "noise trajectories/s", "value": T / wall, "unit": "trajectories/s", "n_gpus": 1, "steps": 1,
+        "metric": "noise trajectories/s", "value": world * T / wall, "unit": "trajectories/s", "n_gpus": world,
+        "steps": 1,
         "warmup": 1, "ms_per_step": wall * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32" if prec == FP32 else "f64", "data": "synthetic",
         "config": {"workload": f"noisy RY/CZ ladder, {n} qubits, depth {depth}, {gates} gates, {len(placements)} "
@@ -328,12 +340,15 @@ def run_trajectories(args) -> None:
                      "model": "per trajectory: 2 x state per fused pass + 1 x state per joint-mass pass"},
         "stats": res.stats, "max_abs_error_vs_other_precision": err,
         "ambiguous_damping_draws": int(res.ambiguous.sum()), "clocks": clocks.summary(),
-        "e2e": {"value": T / wall, "unit": "trajectories/s", "h2d_bytes_per_step": int(rows.nbytes),
-                "d2h_bytes_per_step": int(res.values.nbytes + res.masses.nbytes)},
+        "e2e": {"value": world * T / wall, "unit": "trajectories/s", "h2d_bytes_per_step": int(rows.nbytes) * world,
+                "d2h_bytes_per_step": int(res.values.nbytes + res.masses.nbytes) * world},
         "cpu_baseline": cpu,
     }
+    line["config"]["parallelism"] = f"trajectory partitions x{world}"
     print(json.dumps(line), flush=True)
     ctx.Dispose()
+    if dist is not None:
+        dist.destroy_process_group()
 
 
 def serving_requests(count: int, rate: float, precision: int, seed: int, sessions):
