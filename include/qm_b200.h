@@ -237,6 +237,17 @@ int32_t qm_plan_program(int32_t qubits, int32_t precision, const qm_gate* gates,
                         int32_t max_passes, int32_t* ops, qm_fused_op_info* op_records, int32_t max_ops,
                         int64_t* planned_bytes);
 
+/* Passes compiled for their own op sequence.  Persistent plans (qm_plan_create), the batched
+ * variational evaluator and the trajectory runner compile each distinct pass structure once
+ * (NVRTC for sm_100a; coefficients stay data, so one kernel serves every angle) and run the
+ * compiled kernel; without NVRTC, or with QM_JIT=0 in the environment, they run the
+ * interpreting pass kernel.  qm_jit_info reports whether compilation is available and the
+ * process-wide counts; qm_jit_source returns the generated source of one pass of the plan the
+ * planner makes for `gates` (length receives the full size). */
+int32_t qm_jit_info(int32_t* available, int64_t* kernels, int64_t* failed, int64_t* launches);
+int32_t qm_jit_source(int32_t qubits, int32_t precision, const qm_gate* gates, int32_t count,
+                      int32_t fusion_width, int32_t pass, char* buffer, size_t size, size_t* length);
+
 /* ---------------------------------------------------------------- noise primitives */
 
 /* FP64 compensated masses of target-zero and target-one amplitudes

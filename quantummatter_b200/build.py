@@ -51,7 +51,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         return LIB
     tmp = LIB.with_suffix(".so.tmp")
     cmd = [nvcc(), *ARCH, *FLAGS, "-shared", "-I", str(INCLUDE), "-I", str(CSRC), "-o", str(tmp),
-           *[str(s) for s in sources()], "-cudart", "static", "-lpthread"]
+           *[str(s) for s in sources()], "-cudart", "static", "-lpthread", "-ldl"]
     if verbose:
         print(" ".join(cmd), flush=True)
     res = subprocess.run(cmd, capture_output=True, text=True)

@@ -292,8 +292,8 @@ int32_t run_plan(qm_context* ctx, const Plan& plan, void* amps, const volatile i
             if (rc) return rc;
         }
     } else {
-        for (const FusedPass& p : plan.passes) {
-            QM_CUDA(launch_fused(amps, plan.qubits, plan.precision, p, plan.d_ops, nullptr, ctx->stream));
+        for (size_t i = 0; i < plan.passes.size(); ++i) {
+            QM_CUDA(launch_plan_pass(plan, i, amps, nullptr, ctx->stream));
             int32_t rc = chunk_boundary();
             if (rc) return rc;
         }
@@ -771,6 +771,7 @@ extern "C" int32_t qm_plan_create(qm_context* ctx, int32_t qubits, int32_t preci
     p->ctx = ctx;
     rc = build_plan(ctx, qubits, precision, gates, count, width, p->plan);
     if (rc) { free_plan(p->plan); return rc; }
+    jit_prepare(p->plan);  // a plan is made to be run again: compile its passes once
     QM_CUDA(cudaStreamSynchronize(ctx->stream));
     *out = p.release();
     return QM_OK;

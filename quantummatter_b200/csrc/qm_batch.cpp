@@ -159,8 +159,7 @@ int32_t grow(T*& ptr, size_t& have, size_t need) {
 int32_t enqueue_plan(qm_batch* b, const Plan& plan, int states, const double* d_table, size_t table_stride,
                      cudaStream_t st) {
     FusedBatch fb{states, (uint64_t)1 << b->qubits, d_table, table_stride};
-    for (const FusedPass& p : plan.passes)
-        QM_CUDA(launch_fused(b->amps, b->qubits, b->precision, p, plan.d_ops, &fb, st));
+    for (size_t i = 0; i < plan.passes.size(); ++i) QM_CUDA(launch_plan_pass(plan, i, b->amps, &fb, st));
     return QM_OK;
 }
 
@@ -473,6 +472,7 @@ int32_t vqe_evaluate(qm_context* ctx, int32_t qubits, int32_t precision, const q
         ~Release() { plan_release(p); }
     } release{plan};
     {
+        jit_prepare(plan);  // one structure for every circuit of every wave
         int32_t urc = plan_upload(plan, ctx->stream);
         if (urc) return urc;
     }

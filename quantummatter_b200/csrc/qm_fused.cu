@@ -34,26 +34,6 @@ namespace {
 constexpr int R = kRegBits;
 constexpr int NR = 1 << R;
 
-struct FusedLaunch {
-    uint32_t outer_mask;        // qubits outside the block
-    uint32_t thread_in;         // global mask of the block qubits that are thread bits at load
-    uint32_t thread_out;        // ... at store
-    int32_t op_count;
-    uint32_t reg_in_g[R];       // global bit of each register bit at load
-    uint32_t reg_out_g[R];      // ... at store
-    int32_t reg_in_l[R];        // local positions of the load layout
-    int32_t cta_shift;          // log2 of the CTAs (blocks) per state
-    int32_t states;
-    int32_t table_slots;        // coefficient slots per state (0 without a table)
-    int32_t pad;
-    const FusedOp* ops;         // the pass program in device memory
-    // Batches: state b lives at s + b * state_stride; ops flagged kOpTable take their
-    // coefficients from table + b * table_stride + 8 * op.reserved.
-    const double* table;
-    uint64_t state_stride;
-    uint64_t table_stride;
-};
-
 struct Coef {
     double v[8];
 };
@@ -602,33 +582,7 @@ template <typename T, int K>
 cudaError_t launch_k(void* amps, int qubits, const FusedPass& p, const FusedOp* d_ops, const FusedBatch* batch,
                      cudaStream_t st) {
     using V = typename Vec2<T>::type;
-    FusedLaunch L;
-    const uint32_t all = (1u << qubits) - 1u;
-    L.outer_mask = all & ~p.block_mask;
-    uint32_t reg_in_local = 0, reg_out_local = 0;
-    for (int m = 0; m < R; ++m) {
-        L.reg_in_l[m] = p.reg_in[m];
-        L.reg_in_g[m] = 1u << p.q[p.reg_in[m]];
-        L.reg_out_g[m] = 1u << p.q[p.reg_out[m]];
-        reg_in_local |= 1u << p.reg_in[m];
-        reg_out_local |= 1u << p.reg_out[m];
-    }
-    L.thread_in = 0;
-    L.thread_out = 0;
-    for (int b = 0; b < K; ++b) {
-        if (!(reg_in_local & (1u << b))) L.thread_in |= 1u << p.q[b];
-        if (!(reg_out_local & (1u << b))) L.thread_out |= 1u << p.q[b];
-    }
-    L.op_count = p.op_count;
-    L.ops = d_ops + p.op_begin;
-    L.cta_shift = qubits - K;
-    L.states = batch ? batch->states : 1;
-    const bool tabled = batch && batch->table;
-    L.table = tabled ? batch->table + 8 * (size_t)batch->slot_offset : nullptr;
-    L.state_stride = batch ? batch->state_stride : 0;
-    L.table_stride = batch ? batch->table_stride : 0;
-    L.table_slots = !tabled ? 0 : batch->slot_count >= 0 ? batch->slot_count : (int32_t)(batch->table_stride / 8);
-    L.pad = 0;
+    const FusedLaunch L = fused_launch_params(qubits, p, d_ops, batch);
     const size_t smem = tile_bytes<T, K>() + program_bytes(p.op_count) + sizeof(double) * 8 * (size_t)L.table_slots;
     // device limits and the kernel's shared-memory opt-in, set once per process (thread-safe:
     // several host threads may launch at the same time)
@@ -660,6 +614,38 @@ cudaError_t launch_k(void* amps, int qubits, const FusedPass& p, const FusedOp* 
 }
 
 }  // namespace
+
+FusedLaunch fused_launch_params(int qubits, const FusedPass& p, const FusedOp* d_ops, const FusedBatch* batch) {
+    FusedLaunch L;
+    const int K = p.k;
+    const uint32_t all = (1u << qubits) - 1u;
+    L.outer_mask = all & ~p.block_mask;
+    uint32_t reg_in_local = 0, reg_out_local = 0;
+    for (int m = 0; m < R; ++m) {
+        L.reg_in_l[m] = p.reg_in[m];
+        L.reg_in_g[m] = 1u << p.q[p.reg_in[m]];
+        L.reg_out_g[m] = 1u << p.q[p.reg_out[m]];
+        reg_in_local |= 1u << p.reg_in[m];
+        reg_out_local |= 1u << p.reg_out[m];
+    }
+    L.thread_in = 0;
+    L.thread_out = 0;
+    for (int b = 0; b < K; ++b) {
+        if (!(reg_in_local & (1u << b))) L.thread_in |= 1u << p.q[b];
+        if (!(reg_out_local & (1u << b))) L.thread_out |= 1u << p.q[b];
+    }
+    L.op_count = p.op_count;
+    L.ops = d_ops + p.op_begin;
+    L.cta_shift = qubits - K;
+    L.states = batch ? batch->states : 1;
+    const bool tabled = batch && batch->table;
+    L.table = tabled ? batch->table + 8 * (size_t)batch->slot_offset : nullptr;
+    L.state_stride = batch ? batch->state_stride : 0;
+    L.table_stride = batch ? batch->table_stride : 0;
+    L.table_slots = !tabled ? 0 : batch->slot_count >= 0 ? batch->slot_count : (int32_t)(batch->table_stride / 8);
+    L.pad = 0;
+    return L;
+}
 
 cudaError_t launch_fused(void* amps, int qubits, int precision, const FusedPass& p, const FusedOp* d_ops,
                          const FusedBatch* batch, cudaStream_t st) {

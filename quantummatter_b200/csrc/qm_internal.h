@@ -108,6 +108,7 @@ struct Plan {
     std::vector<FusedPass> passes;  // fused path
     std::vector<FusedOp> ops;
     FusedOp* d_ops = nullptr;       // device copy of ops (each pass's program is staged from it)
+    std::vector<const void*> jit;   // per pass: compiled kernel (cudaKernel_t) or null
     bool borrowed = false;          // d_ops belongs to a context buffer
     int64_t planned_bytes = 0;
     int32_t launches = 0;
@@ -141,6 +142,35 @@ struct FusedBatch {
 };
 cudaError_t launch_fused(void* amps, int qubits, int precision, const FusedPass& p, const FusedOp* ops,
                          const FusedBatch* batch, cudaStream_t s);
+
+// Kernel parameters of a fused pass (the interpreter k_fused and the passes compiled for their
+// own op sequence take the same struct; its layout is mirrored in the compiled source).
+struct FusedLaunch {
+    uint32_t outer_mask;        // qubits outside the block
+    uint32_t thread_in;         // global mask of the block qubits that are thread bits at load
+    uint32_t thread_out;        // ... at store
+    int32_t op_count;
+    uint32_t reg_in_g[kRegBits];  // global bit of each register bit at load
+    uint32_t reg_out_g[kRegBits]; // ... at store
+    int32_t reg_in_l[kRegBits];   // local positions of the load layout
+    int32_t cta_shift;          // log2 of the CTAs (blocks) per state
+    int32_t states;
+    int32_t table_slots;        // coefficient slots per state (0 without a table)
+    int32_t pad;
+    const FusedOp* ops;         // the pass program in device memory
+    // Batches: state b lives at s + b * state_stride; ops flagged kOpTable take their
+    // coefficients from table + b * table_stride + 8 * op.reserved.
+    const double* table;
+    uint64_t state_stride;
+    uint64_t table_stride;
+};
+FusedLaunch fused_launch_params(int qubits, const FusedPass& p, const FusedOp* d_ops, const FusedBatch* batch);
+
+// Passes compiled for their own op sequence (qm_jit.cpp).  A plan's passes are compiled by
+// jit_prepare (NVRTC, sm_100a; structurally equal passes share a kernel); launch_plan_pass runs
+// a pass with its compiled kernel when there is one, else with k_fused.
+void jit_prepare(Plan& plan);
+cudaError_t launch_plan_pass(const Plan& plan, size_t pass, void* amps, const FusedBatch* batch, cudaStream_t s);
 cudaError_t launch_reset(void* amps, int qubits, int precision, cudaStream_t s);
 cudaError_t launch_convert_from_f64(void* dst_f32, const double* src_f64, int64_t n, cudaStream_t s);
 cudaError_t launch_convert_to_f64(double* dst_f64, const void* src_f32, int64_t n, cudaStream_t s);
