@@ -516,7 +516,7 @@ def main() -> None:
     import numpy as np
 
     from quantummatter_b200.backend import (FP32, FP64, B200BackendOptions, B200Context, B200StateVectorBackend,
-                                            DeviceState, Plan)
+                                            DeviceState, Plan, jit_info)
     from quantummatter_b200.workloads import brick_circuit
 
     qubits, depth = args.qubits, args.depth
@@ -536,12 +536,14 @@ def main() -> None:
         plan.execute(state)
     barrier_max(dist, 0.0, local)
     device_seconds = []
+    jit_before = jit_info()["launches"]
     with ClockSampler(local) as clocks:
         t_wall = time.perf_counter()
         for _ in range(args.steps):
             prof = plan.execute(state, profile=True)
             device_seconds.append(prof.DeviceEvolutionSeconds)
         wall = time.perf_counter() - t_wall
+    compiled = jit_info()["launches"] - jit_before == args.steps * launches and passes > 0
     total = sum(device_seconds)
     total_max = barrier_max(dist, total, local)
     ms_per_step = 1e3 * total_max / args.steps
@@ -552,8 +554,9 @@ def main() -> None:
     per_launch_s = total / (args.steps * launches)
     bytes_per_launch = planned_bytes / launches
     achieved_gbs = bytes_per_launch / per_launch_s / 1e9
-    kernel_key = f"k_fused_{args.precision}_k{plan_width(passes, qubits, precision, args.width)}_{qubits}q" if passes else \
-        f"k_gate_{args.precision}_{qubits}q"
+    # the pass kernel that ran: compiled for each pass's op sequence (qm_pass) or the interpreter
+    kernel_key = f"{'qm_pass' if compiled else 'k_fused'}_{args.precision}_k{plan_width(passes, qubits, precision, args.width)}_{qubits}q" \
+        if passes else f"k_gate_{args.precision}_{qubits}q"
     traffic = profile_traffic(kernel_key)
 
     # FP64/FP32 arithmetic actually issued: 16 real FMA-flops per amplitude per dense 2x2 gate

@@ -405,3 +405,12 @@ class DeviceState:
         check(load().qm_sample(self.handle, d.ctypes.data_as(_lib.DP), d.size, out.ctypes.data_as(_lib.I64P),
                                C.byref(amb)))
         return out, amb.value
+
+
+def jit_info() -> dict:
+    """Whether passes can be compiled for their own op sequence, and process-wide counts of
+    compiled kernels, failed compilations and launches of compiled passes (qm_jit_info)."""
+    avail, kernels, failed, launches = C.c_int32(), C.c_int64(), C.c_int64(), C.c_int64()
+    check(load().qm_jit_info(C.byref(avail), C.byref(kernels), C.byref(failed), C.byref(launches)))
+    return {"available": bool(avail.value), "kernels": kernels.value, "failed": failed.value,
+            "launches": launches.value}

@@ -267,6 +267,9 @@ int32_t build_plan(qm_context* ctx, int32_t qubits, int32_t precision, const qm_
     std::string err;
     if (width == 0) width = ctx->fusion_width;
     if (!plan_fused(list, qubits, precision, width, plan, err)) return fail(QM_E_ARG, "planner: " + err);
+    // one-shot executions of large states run the compiled passes already built for the same
+    // structures; they never wait for a compilation
+    if (transient && qubits >= 20) jit_lookup(plan);
     if (transient) return plan_upload(plan, ctx->stream, &ctx->program, &ctx->program_bytes);
     return plan_upload(plan, ctx->stream);
 }

@@ -170,6 +170,7 @@ FusedLaunch fused_launch_params(int qubits, const FusedPass& p, const FusedOp* d
 // jit_prepare (NVRTC, sm_100a; structurally equal passes share a kernel); launch_plan_pass runs
 // a pass with its compiled kernel when there is one, else with k_fused.
 void jit_prepare(Plan& plan);
+void jit_lookup(Plan& plan);  // compiled kernels already in the cache only (no compilation)
 cudaError_t launch_plan_pass(const Plan& plan, size_t pass, void* amps, const FusedBatch* batch, cudaStream_t s);
 cudaError_t launch_reset(void* amps, int qubits, int precision, cudaStream_t s);
 cudaError_t launch_convert_from_f64(void* dst_f32, const double* src_f64, int64_t n, cudaStream_t s);

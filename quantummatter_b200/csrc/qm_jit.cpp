@@ -598,6 +598,21 @@ void jit_prepare(Plan& plan) {
     for (size_t i = 0; i < src.size(); ++i) plan.jit[i] = reinterpret_cast<const void*>(kernel_for(src[i]));
 }
 
+void jit_lookup(Plan& plan) {
+    plan.jit.assign(plan.passes.size(), nullptr);
+    if (!jit_enabled() || plan.passes.empty()) return;
+    {
+        std::lock_guard<std::mutex> lock(g_cache_mu);
+        if (g_cache.empty()) return;
+    }
+    const bool fp64 = plan.precision != QM_FP32;
+    std::lock_guard<std::mutex> lock(g_cache_mu);
+    for (size_t i = 0; i < plan.passes.size(); ++i) {
+        auto it = g_cache.find(generate(plan.passes[i], plan.ops, fp64));
+        if (it != g_cache.end() && !it->second.failed) plan.jit[i] = reinterpret_cast<const void*>(it->second.kernel);
+    }
+}
+
 cudaError_t launch_plan_pass(const Plan& plan, size_t pass, void* amps, const FusedBatch* batch, cudaStream_t st) {
     const FusedPass& p = plan.passes[pass];
     const void* kernel = pass < plan.jit.size() ? plan.jit[pass] : nullptr;
