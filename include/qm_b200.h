@@ -292,6 +292,18 @@ int32_t qm_measure_all(qm_state* state, double u, int64_t* outcome, int32_t* amb
  * search per shot, without collapse.  *ambiguous counts shots near a boundary. */
 int32_t qm_sample(qm_state* state, const double* draws, int32_t shots, int64_t* outcomes,
                   int32_t* ambiguous);
+/* StateVector.MarginalProbability (src/QuantumMatter.Core/StateVector.Observations.cs:10-36): the
+ * normalised Born probability that qubits[k] reads bit k of `outcome`, for all k.  Selections
+ * are 1..qubits distinct in-range qubits (QM_E_ARG / QM_E_RANGE otherwise). */
+int32_t qm_marginal_probability(qm_state* state, const int32_t* qubits, int32_t count, int32_t outcome,
+                                double* probability);
+/* StateVector.Measure (StateVector.Observations.cs:38-97): one full-basis Born draw (u is the
+ * caller's NextDouble), then the state is projected onto the drawn values of the selected qubits
+ * and renormalised, keeping the surviving phases.  Bit k of *outcome is qubits[k]'s value;
+ * *ambiguous is set when u * total lies within the rounding margin of a CDF boundary.  The state
+ * stays on the device: dynamic circuits keep their classical control on the host. */
+int32_t qm_measure(qm_state* state, const int32_t* qubits, int32_t count, double u, int32_t* outcome,
+                   int32_t* ambiguous);
 
 /* ---------------------------------------------------------------- batches */
 

@@ -248,6 +248,33 @@ def measure_all(state: np.ndarray, u: float) -> tuple[np.ndarray, int]:
     return s, out.value
 
 
+def marginal_probability(state: np.ndarray, qubits: Sequence[int], outcome: int) -> float:
+    sel = (C.c_int32 * len(qubits))(*qubits)
+    out = C.c_double()
+    lib = load()
+    lib.qmo_marginal_probability.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.c_int32, C.c_int32,
+                                             C.POINTER(C.c_double)]
+    s = np.ascontiguousarray(state, dtype=np.complex128)
+    rc = lib.qmo_marginal_probability(_buf(s), int(np.log2(s.size)), sel, len(qubits), outcome, C.byref(out))
+    if rc:
+        raise RuntimeError(f"oracle marginal failed: {rc}")
+    return out.value
+
+
+def measure(state: np.ndarray, qubits: Sequence[int], u: float) -> tuple[np.ndarray, int]:
+    """StateVector.Measure on a copy: (projected state, outcome)."""
+    sel = (C.c_int32 * len(qubits))(*qubits)
+    out = C.c_int32()
+    lib = load()
+    lib.qmo_measure.argtypes = [C.c_void_p, C.c_int32, C.POINTER(C.c_int32), C.c_int32, C.c_double,
+                                C.POINTER(C.c_int32)]
+    s = np.array(state, dtype=np.complex128, copy=True)
+    rc = lib.qmo_measure(_buf(s), int(np.log2(s.size)), sel, len(qubits), u, C.byref(out))
+    if rc:
+        raise RuntimeError(f"oracle measure failed: {rc}")
+    return s, out.value
+
+
 class DotNetRandom:
     """Seeded System.Random stand-in (restated subtractive generator; see qm_oracle.c)."""
 

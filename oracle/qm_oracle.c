@@ -486,6 +486,76 @@ int qmo_measure_all(double* s, int32_t qubits, double u, int64_t* outcome) {
     return 0;
 }
 
+/* StateVector.MarginalProbability (src/QuantumMatter.Core/StateVector.Observations.cs:10-36):
+ * plain sequential sums of the total and the selected Born masses.  Bit k of outcome refers to
+ * qubits[k].  Returns 0, 1 for a bad selection, 7 for no finite positive mass. */
+int qmo_marginal_probability(const double* s, int32_t nq, const int32_t* qubits, int32_t count, int32_t outcome,
+                             double* probability) {
+    int64_t len = (int64_t)1 << nq, mask = 0, pattern = 0;
+    if (count < 1 || count > nq) return 1;
+    for (int32_t k = 0; k < count; ++k) {
+        if (qubits[k] < 0 || qubits[k] >= nq || (mask >> qubits[k]) & 1) return 1;
+        mask |= (int64_t)1 << qubits[k];
+        pattern |= (int64_t)((outcome >> k) & 1) << qubits[k];
+    }
+    double total = 0, selected = 0;
+    for (int64_t i = 0; i < len; ++i) {
+        cpx v = ld(s, i);
+        double prob = v.re * v.re + v.im * v.im;
+        total += prob;
+        if ((i & mask) == pattern) selected += prob;
+    }
+    if (!isfinite(total) || total <= 0) return 7;
+    *probability = selected / total;
+    return 0;
+}
+
+/* StateVector.Measure (StateVector.Observations.cs:38-97): one full-basis Born draw with the
+ * strict upper-bound search, the matching branch's mass, then the projection (matching
+ * amplitudes divided by the square root of that mass, the rest zero). */
+int qmo_measure(double* s, int32_t nq, const int32_t* qubits, int32_t count, double u, int32_t* outcome) {
+    int64_t len = (int64_t)1 << nq, mask = 0;
+    if (count < 1 || count > nq) return 1;
+    for (int32_t k = 0; k < count; ++k) {
+        if (qubits[k] < 0 || qubits[k] >= nq || (mask >> qubits[k]) & 1) return 1;
+        mask |= (int64_t)1 << qubits[k];
+    }
+    double total = 0;
+    int64_t last = -1;
+    for (int64_t i = 0; i < len; ++i) {
+        cpx v = ld(s, i);
+        double prob = v.re * v.re + v.im * v.im;
+        total += prob;
+        if (prob > 0) last = i;
+    }
+    if (!isfinite(total) || total <= 0) return 7;
+    double draw = u * total, cumulative = 0;
+    int64_t basis = last;
+    for (int64_t i = 0; i < len; ++i) {
+        cpx v = ld(s, i);
+        cumulative += v.re * v.re + v.im * v.im;
+        if (draw < cumulative) { basis = i; break; }
+    }
+    int64_t pattern = basis & mask;
+    double branch = 0;
+    for (int64_t i = 0; i < len; ++i) {
+        if ((i & mask) != pattern) continue;
+        cpx v = ld(s, i);
+        branch += v.re * v.re + v.im * v.im;
+    }
+    if (!isfinite(branch) || branch <= 0) return 7;
+    double norm = sqrt(branch);
+    for (int64_t i = 0; i < len; ++i) {
+        cpx v = ld(s, i);
+        if ((i & mask) == pattern) st(s, i, mk(v.re / norm, v.im / norm));
+        else st(s, i, mk(0, 0));
+    }
+    int32_t out = 0;
+    for (int32_t k = 0; k < count; ++k) out |= (int32_t)((basis >> qubits[k]) & 1) << k;
+    *outcome = out;
+    return 0;
+}
+
 /* ---------------------------------------------------------------- System.Random */
 
 /* Seeded System.Random: Knuth's subtractive generator (Numerical Recipes "ran3"),

@@ -97,6 +97,9 @@ int qmo_trajectory(const qmo_operation* ops, int32_t count, const qmo_channel* c
 /* ---- sampling ---- */
 int qmo_sample(const double* amps, int32_t qubits, const double* draws, int32_t shots, int64_t* out);
 int qmo_measure_all(double* amps, int32_t qubits, double draw, int64_t* outcome);
+int qmo_marginal_probability(const double* amps, int32_t qubits, const int32_t* selection, int32_t count,
+                             int32_t outcome, double* probability);
+int qmo_measure(double* amps, int32_t qubits, const int32_t* selection, int32_t count, double draw, int32_t* outcome);
 
 /* ---- System.Random (seeded) restatement ---- */
 typedef struct qmo_random { int32_t seed_array[56]; int32_t inext, inextp; } qmo_random;

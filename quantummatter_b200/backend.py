@@ -396,6 +396,21 @@ class DeviceState:
         check(load().qm_measure_all(self.handle, float(u), C.byref(out), C.byref(amb)))
         return out.value, bool(amb.value)
 
+    def MarginalProbability(self, qubits: Sequence[int], outcome: int) -> float:
+        """StateVector.MarginalProbability: bit k of outcome refers to qubits[k]."""
+        sel = (C.c_int32 * max(1, len(qubits)))(*qubits)
+        p = C.c_double()
+        check(load().qm_marginal_probability(self.handle, sel, len(qubits), int(outcome), C.byref(p)))
+        return p.value
+
+    def Measure(self, qubits: Sequence[int], u: float) -> tuple[int, bool]:
+        """StateVector.Measure with the draw u: projects the state on the device and returns the
+        selected qubits' values (bit k = qubits[k]) and whether u sat on a CDF boundary."""
+        sel = (C.c_int32 * max(1, len(qubits)))(*qubits)
+        out, amb = C.c_int32(), C.c_int32()
+        check(load().qm_measure(self.handle, sel, len(qubits), float(u), C.byref(out), C.byref(amb)))
+        return out.value, bool(amb.value)
+
     def Sample(self, draws: Sequence[float]) -> tuple[np.ndarray, int]:
         d = np.ascontiguousarray(draws, dtype=np.float64)
         if d.size < 1:

@@ -1130,6 +1130,90 @@ extern "C" int32_t qm_sample(qm_state* st, const double* draws, int32_t shots, i
     return device_sample(st, draws, shots, outcomes, ambiguous);
 }
 
+namespace {
+
+// StateVector.ValidateSelection (StateVector.Observations.cs:143-168): the mask of the selection.
+int32_t selection_mask(const int32_t* qubits, int32_t count, int32_t register_qubits, uint64_t* mask) {
+    if (!qubits || count < 1 || count > register_qubits)
+        return fail(QM_E_ARG, "Select between one and QubitCount distinct qubits.");
+    uint64_t m = 0;
+    for (int32_t k = 0; k < count; ++k) {
+        if ((uint32_t)qubits[k] >= (uint32_t)register_qubits) return fail(QM_E_RANGE, "Selected qubits must be in range.");
+        const uint64_t bit = 1ull << qubits[k];
+        if (m & bit) return fail(QM_E_ARG, "Selected qubits must be distinct.");
+        m |= bit;
+    }
+    *mask = m;
+    return QM_OK;
+}
+
+// (selected, total) Born masses on the device, FP64 compensated.
+int32_t pattern_masses(qm_state* st, uint64_t mask, uint64_t pattern, double* selected, double* total) {
+    qm_context* ctx = st->ctx;
+    int32_t rc = ensure_scratch(ctx, sizeof(double) * (4 * 148 * 4 + 8));
+    if (rc) return rc;
+    rc = ensure_host_scratch(ctx, 4 * sizeof(double));
+    if (rc) return rc;
+    double* partial = static_cast<double*>(ctx->scratch);
+    int blocks = 0;
+    QM_CUDA(launch_pattern_masses(st->amps, st->qubits, st->precision, mask, pattern, partial, &blocks, ctx->stream));
+    double* out = partial + 4 * blocks;
+    QM_CUDA(launch_finish_sums(partial, blocks, 4, out, ctx->stream));
+    QM_CUDA(cudaMemcpyAsync(ctx->host_scratch, out, 4 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    QM_CUDA(cudaStreamSynchronize(ctx->stream));
+    *selected = ctx->host_scratch[0] + ctx->host_scratch[1];
+    *total = ctx->host_scratch[2] + ctx->host_scratch[3];
+    return QM_OK;
+}
+
+}  // namespace
+
+extern "C" int32_t qm_marginal_probability(qm_state* st, const int32_t* qubits, int32_t count, int32_t outcome,
+                                           double* probability) {
+    int32_t rc = check_state(st);
+    if (rc) return rc;
+    if (!probability) return fail(QM_E_ARG, "probability is null");
+    uint64_t mask = 0;
+    if ((rc = selection_mask(qubits, count, st->qubits, &mask))) return rc;
+    if (outcome < 0 || (count < 31 && outcome >= (1 << count))) return fail(QM_E_RANGE, "outcome out of range");
+    uint64_t pattern = 0;
+    for (int32_t k = 0; k < count; ++k) pattern |= (uint64_t)((outcome >> k) & 1) << qubits[k];
+    std::lock_guard<std::recursive_mutex> lock(st->ctx->mu);
+    QM_CUDA(cudaSetDevice(st->ctx->device));
+    double selected = 0, total = 0;
+    if ((rc = pattern_masses(st, mask, pattern, &selected, &total))) return rc;
+    if (!std::isfinite(total) || total <= 0) return fail(QM_E_MASS, "The state has no finite positive probability mass.");
+    *probability = selected / total;
+    return QM_OK;
+}
+
+extern "C" int32_t qm_measure(qm_state* st, const int32_t* qubits, int32_t count, double u, int32_t* outcome,
+                              int32_t* ambiguous) {
+    int32_t rc = check_state(st);
+    if (rc) return rc;
+    if (!outcome) return fail(QM_E_ARG, "outcome is null");
+    uint64_t mask = 0;
+    if ((rc = selection_mask(qubits, count, st->qubits, &mask))) return rc;
+    if (!std::isfinite(u) || u < 0 || u >= 1) return fail(QM_E_RANGE, "draw must be in [0,1)");
+    std::lock_guard<std::recursive_mutex> lock(st->ctx->mu);
+    QM_CUDA(cudaSetDevice(st->ctx->device));
+    // one full-basis Born draw (the device CDF and search of qm_sample)
+    int64_t basis = -1;
+    int32_t amb = 0;
+    if ((rc = device_sample(st, &u, 1, &basis, &amb))) return rc;
+    const uint64_t pattern = (uint64_t)basis & mask;
+    double branch = 0, total = 0;
+    if ((rc = pattern_masses(st, mask, pattern, &branch, &total))) return rc;
+    if (!std::isfinite(branch) || branch <= 0) return fail(QM_E_MASS, "The state has no finite positive probability mass.");
+    QM_CUDA(launch_project(st->amps, st->qubits, st->precision, mask, pattern, std::sqrt(branch), st->ctx->stream));
+    QM_CUDA(cudaStreamSynchronize(st->ctx->stream));
+    int32_t out = 0;
+    for (int32_t k = 0; k < count; ++k) out |= (int32_t)((basis >> qubits[k]) & 1) << k;
+    *outcome = out;
+    if (ambiguous) *ambiguous = amb;
+    return QM_OK;
+}
+
 extern "C" int32_t qm_measure_all(qm_state* st, double u, int64_t* outcome, int32_t* ambiguous) {
     int32_t rc = check_state(st);
     if (rc) return rc;

@@ -201,6 +201,12 @@ cudaError_t launch_search(const void* amps, int qubits, int precision, const dou
                           int blocks, int chunk, const double* targets, int shots, double margin,
                           int64_t* out, cudaStream_t s);
 cudaError_t launch_collapse(void* amps, int qubits, int precision, int64_t outcome, cudaStream_t s);
+// (selected sum, compensation, total sum, compensation) per block for amplitudes with
+// (index & mask) == pattern; blocks = expectation_blocks(qubits).
+cudaError_t launch_pattern_masses(const void* amps, int qubits, int precision, uint64_t mask, uint64_t pattern,
+                                  double* scratch, int* blocks_out, cudaStream_t s);
+cudaError_t launch_project(void* amps, int qubits, int precision, uint64_t mask, uint64_t pattern, double norm,
+                           cudaStream_t s);
 
 // ---------------------------------------------------------------- tiled expectation (qm_expect.cu)
 constexpr int kTileMaxTerms = 256;

@@ -414,6 +414,48 @@ __global__ void k_search(const typename Vec2<T>::type* __restrict__ s, const dou
     }
 }
 
+// Born masses of the amplitudes whose masked bits equal `pattern` and of all amplitudes
+// (StateVector.MarginalProbability and Measure's branch mass, StateVector.Observations.cs:10-88):
+// compensated FP64 per thread, deterministic block tree, (selected, total) per block.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_pattern_masses(const typename Vec2<T>::type* __restrict__ s, uint64_t n,
+                                                             uint64_t mask, uint64_t pattern, double* out) {
+    __shared__ KSum red[kThreads / 32];
+    KSum sel{0, 0}, tot{0, 0};
+    for (uint64_t i = (uint64_t)blockIdx.x * kThreads + threadIdx.x; i < n; i += (uint64_t)gridDim.x * kThreads) {
+        const Cx<T> x = load_amp<T>(s, i);
+        const double xr = x.re, xi = x.im;
+        const double p = xr * xr + xi * xi;
+        tot.add(p);
+        if ((i & mask) == pattern) sel.add(p);
+    }
+    KSum st = block_reduce_ksum(sel, red);
+    KSum tt = block_reduce_ksum(tot, red);
+    if (threadIdx.x == 0) {
+        out[4 * blockIdx.x + 0] = st.s;
+        out[4 * blockIdx.x + 1] = st.c;
+        out[4 * blockIdx.x + 2] = tt.s;
+        out[4 * blockIdx.x + 3] = tt.c;
+    }
+}
+
+// Measure's projection (StateVector.Observations.cs:86-93): the matching branch divided by the
+// square root of its mass, every other amplitude zero.
+template <typename T>
+__global__ void k_project(typename Vec2<T>::type* s, uint64_t n, uint64_t mask, uint64_t pattern, double norm) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        Cx<T> x = load_amp<T>(s, i);
+        if ((i & mask) == pattern) {
+            x.re = (T)((double)x.re / norm);
+            x.im = (T)((double)x.im / norm);
+        } else {
+            x.re = (T)0;
+            x.im = (T)0;
+        }
+        store_amp<T>(s, i, x);
+    }
+}
+
 template <typename T>
 __global__ void k_collapse(typename Vec2<T>::type* s, uint64_t n, uint64_t outcome) {
     uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -597,6 +639,28 @@ cudaError_t launch_search(const void* amps, int qubits, int precision, const dou
     else
         k_search<double><<<grid, threads, 0, st>>>((const double2*)amps, prefix, blocks, (uint32_t)chunk, targets, shots,
                                                    margin, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pattern_masses(const void* amps, int qubits, int precision, uint64_t mask, uint64_t pattern,
+                                  double* scratch, int* blocks_out, cudaStream_t st) {
+    const uint64_t n = 1ull << qubits;
+    const int blocks = reduce_blocks(n);
+    *blocks_out = blocks;
+    if (precision == QM_FP32)
+        k_pattern_masses<float><<<blocks, kThreads, 0, st>>>((const float2*)amps, n, mask, pattern, scratch);
+    else
+        k_pattern_masses<double><<<blocks, kThreads, 0, st>>>((const double2*)amps, n, mask, pattern, scratch);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_project(void* amps, int qubits, int precision, uint64_t mask, uint64_t pattern, double norm,
+                           cudaStream_t st) {
+    const uint64_t n = 1ull << qubits;
+    if (precision == QM_FP32)
+        k_project<float><<<stream_blocks(n), kThreads, 0, st>>>((float2*)amps, n, mask, pattern, norm);
+    else
+        k_project<double><<<stream_blocks(n), kThreads, 0, st>>>((double2*)amps, n, mask, pattern, norm);
     return cudaGetLastError();
 }
 
