@@ -72,10 +72,15 @@ __global__ void __launch_bounds__(1 << (K - R), 512 / (1 << (K - R)))
     }
     __syncthreads();
 
-    // Terms arrive sorted by flip mask; up to kGroup consecutive terms with the same mask share
-    // one partner load and one overlap per amplitude.
+    // Terms arrive sorted by flip mask, the diagonal ones (flip 0) first.  Three or more
+    // diagonal terms are evaluated together through a Walsh-Hadamard transform of the tile's
+    // Born probabilities (below); the rest in groups of up to kGroup consecutive terms with the
+    // same mask, which share one partner load and one overlap per amplitude.
+    int ndiag = 0;
+    while (ndiag < P.terms && P.t[ndiag].flip_local == 0) ++ndiag;
+    const bool wht = ndiag >= 3;
     constexpr int kGroup = 4;
-    for (int k = 0; k < P.terms;) {
+    for (int k = wht ? ndiag : 0; k < P.terms;) {
         const uint32_t flip = P.t[k].flip_local;
         int cnt = 1;
         while (cnt < kGroup && k + cnt < P.terms && P.t[k + cnt].flip_local == flip) ++cnt;
@@ -132,10 +137,71 @@ __global__ void __launch_bounds__(1 << (K - R), 512 / (1 << (K - R)))
         acc = warp_sum(acc);
         if (lane == 0) red[warp * (P.terms + 1) + P.terms] = acc;
     }
+    // Walsh-Hadamard transform over the tile's local bits: W[S] = sum_j |psi_j|^2 (-1)^popc(j & S),
+    // so a diagonal term with local sign mask S is W[S] times the sign of its bits outside the
+    // tile.  Register bits in registers, lane bits through shuffles, warp bits through shared
+    // memory (the tile, no longer needed), all in a fixed order.
+    double* wbuf = reinterpret_cast<double*>(smem_raw);
+    if (wht) {
+        double w[NR];
+#pragma unroll
+        for (int i = 0; i < NR; ++i) {
+            const V a = tile[t | ((uint32_t)i << (K - R))];
+            w[i] = (double)a.x * a.x + (double)a.y * a.y;
+        }
+#pragma unroll
+        for (int m = 0; m < R; ++m)
+#pragma unroll
+            for (int i = 0; i < NR; ++i)
+                if (!((i >> m) & 1)) {
+                    const double x = w[i], y = w[i | (1 << m)];
+                    w[i] = x + y;
+                    w[i | (1 << m)] = x - y;
+                }
+#pragma unroll
+        for (int m = 0; m < 5; ++m)
+#pragma unroll
+            for (int i = 0; i < NR; ++i) {
+                const double y = __shfl_xor_sync(0xffffffffu, w[i], 1 << m);
+                w[i] = ((lane >> m) & 1) ? y - w[i] : w[i] + y;
+            }
+        __syncthreads();  // every read of the tile is done
+#pragma unroll
+        for (int i = 0; i < NR; ++i) wbuf[t | ((uint32_t)i << (K - R))] = w[i];
+#pragma unroll
+        for (int m = 5; m < K - R; ++m) {
+            __syncthreads();
+#pragma unroll
+            for (int i = 0; i < NR; ++i) {
+                const uint32_t j = t | ((uint32_t)i << (K - R));
+                const double x = wbuf[j], y = wbuf[j ^ (1u << m)];
+                w[i] = ((j >> m) & 1u) ? y - x : x + y;
+            }
+            __syncthreads();
+#pragma unroll
+            for (int i = 0; i < NR; ++i) wbuf[t | ((uint32_t)i << (K - R))] = w[i];
+        }
+    }
     __syncthreads();
     const size_t row = (size_t)blockIdx.y * P.rows_per_state + P.row_offset + blockIdx.x;
     for (int k = t; k < P.terms + (P.with_mass ? 1 : 0); k += NT) {
         double sum = 0.0;
+        if (wht && k < ndiag) {
+            const uint32_t sg = P.t[k].sign;
+            uint32_t loc = 0, tm = P.thread_mask;
+            for (int b = 0; tm; ++b) {
+                const uint32_t low = tm & (0u - tm);
+                if (sg & low) loc |= 1u << b;
+                tm ^= low;
+            }
+#pragma unroll
+            for (int m = 0; m < R; ++m)
+                if (sg & P.reg_g[m]) loc |= 1u << (K - R + m);
+            sum = wbuf[loc];
+            if (__popc(sg & outer) & 1) sum = -sum;
+            P.partials[row * P.columns + P.t[k].column] = sum;
+            continue;
+        }
         for (int w = 0; w < WARPS; ++w) sum += red[w * (P.terms + 1) + k];
         const int col = k < P.terms ? P.t[k].column : P.mass_column;
         P.partials[row * P.columns + col] = sum;
