@@ -487,6 +487,8 @@ def main() -> None:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="brick", choices=["brick", "vqe", "trajectories", "serving"])
+    ap.add_argument("--circuit", default="brick", choices=["brick", "qft", "grover"],
+                    help="brick workload: the circuit (qft and grover: the algorithm builders at --qubits)")
     ap.add_argument("--sizes", default="16,18,20,22", help="vqe workload: qubit counts")
     ap.add_argument("--vectors", type=int, default=128, help="vqe workload: parameter vectors per size")
     ap.add_argument("--traj-qubits", type=int, default=24, help="trajectories workload: qubits")
@@ -517,12 +519,24 @@ def main() -> None:
 
     from quantummatter_b200.backend import (FP32, FP64, B200BackendOptions, B200Context, B200StateVectorBackend,
                                             DeviceState, Plan, jit_info)
+    from quantummatter_b200.algorithms import GroverSearch, QuantumFourierTransform
     from quantummatter_b200.workloads import brick_circuit
 
     qubits, depth = args.qubits, args.depth
     precision = FP32 if args.precision == "fp32" else FP64
     elem = 8 if precision == FP32 else 16
-    circuit = brick_circuit(qubits, depth)
+    if args.circuit == "qft":
+        circuit = QuantumFourierTransform.CreateCircuit(qubits)
+        described = f"quantum Fourier transform, {qubits} qubits (H, controlled phases, bit-reversal swaps)"
+    elif args.circuit == "grover":
+        inputs = (qubits + 2) // 2
+        circuit = GroverSearch.CreateCircuit(inputs, (1 << inputs) // 3, iterations=2)
+        qubits = circuit.QubitCount
+        described = (f"Grover search, {inputs} input + {qubits - inputs} scratch qubits, 2 iterations "
+                     f"(X, H, Toffoli ladders, CZ)")
+    else:
+        circuit = brick_circuit(qubits, depth)
+        described = f"brick circuit, {qubits} qubits, depth {depth}, U3 + CNOT"
     gates = len(circuit.Operations)
     amps = 1 << qubits
     ctx = B200Context(B200BackendOptions(DeviceIndex=local, DeviceMemoryBudgetBytes=80 << 30,
@@ -559,8 +573,9 @@ def main() -> None:
         if passes else f"k_gate_{args.precision}_{qubits}q"
     traffic = profile_traffic(kernel_key)
 
-    # FP64/FP32 arithmetic actually issued: 16 real FMA-flops per amplitude per dense 2x2 gate
-    dense = sum(1 for op in circuit.Operations if int(op.Kind) not in (1, 9, 10, 11, 16))
+    # FP64/FP32 arithmetic of the dense 2x2 gates (H, Rx, Ry, Unitary): 16 real flops per amplitude;
+    # permutations and diagonal phases are counted as free
+    dense = sum(1 for op in circuit.Operations if int(op.Kind) in (0, 6, 7, 15))
     flops = dense * amps * 8 * 2
     e2e = None
     if not args.no_e2e and precision == FP64:
@@ -587,11 +602,11 @@ def main() -> None:
 
     if rank == 0:
         line = {
-            "metric": "amp-updates/s at 30q", "value": value, "unit": "amp-updates/s", "n_gpus": world,
+            "metric": f"amp-updates/s at {qubits}q", "value": value, "unit": "amp-updates/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32" if precision == FP32 else "f64",
             "data": "synthetic",
-            "config": {"workload": f"brick circuit, {qubits} qubits, depth {depth}, U3 + CNOT, {gates} gates, "
+            "config": {"workload": f"{described}, {gates} gates, "
                                    f"{'complex64' if precision == FP32 else 'complex128'} state resident in HBM",
                        "qubits": qubits, "depth": depth, "gates": gates, "precision": args.precision,
                        "fusion": f"{passes} fused passes (block width {plan_width(passes, qubits, precision, args.width)})"
