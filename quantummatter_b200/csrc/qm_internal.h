@@ -109,6 +109,7 @@ struct Plan {
     std::vector<FusedOp> ops;
     FusedOp* d_ops = nullptr;       // device copy of ops (each pass's program is staged from it)
     std::vector<const void*> jit;   // per pass: compiled kernel (cudaKernel_t) or null
+    std::vector<std::vector<unsigned char>> jit_aux;  // per pass: the compiled kernel's constants
     bool borrowed = false;          // d_ops belongs to a context buffer
     int64_t planned_bytes = 0;
     int32_t launches = 0;

@@ -19,6 +19,8 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cmath>
+#include <complex>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
@@ -115,6 +117,95 @@ std::string deposit_expr(const char* value, uint32_t mask) {
     return e.str();
 }
 
+// ---------------------------------------------------------------- deferred phases
+// An uncontrolled 2x2 unitary is applied as
+//     U = g diag(1, phi) m R diag(1, lam),  R = [[1, -t], [t, 1]] (|u00| >= |u10|) or [[t, -1], [1, t]],
+// with |t| <= 1 and g, phi, lam of unit modulus.  On a register pair (x, y) that is
+// w = lam y; x' = x - t w; y' = t x + w (or x' = t x - w; y' = x + t w): 8 flops against 16 for the
+// dense product.  The scalar g m and the phase phi are deferred: phi becomes a pending phase
+// exp(i theta parity(S)) over a set S of qubits, which the next rotation on a qubit of S takes
+// into its lam, which an X or CNOT rewrites (conjugate; S xor {control}), and which the plan's
+// last pass multiplies in.  Other passes only rescale by |g m| so magnitudes stay bounded.
+using cplx = std::complex<double>;
+
+struct Split {
+    bool ok = false;
+    bool form_b = false;  // R = [[t, -1], [1, t]]
+    double t = 0.0;
+    cplx gm{1.0, 0.0};
+    cplx lam{1.0, 0.0}, phi{1.0, 0.0};
+};
+
+// The split of a 2x2 matrix (a, b, c, d as re/im pairs); ok only when it gives the matrix back
+// to within 1e-15 in every entry (a unitary to double precision), so results stay those of the
+// dense product to rounding.
+Split split_unitary(const double* c) {
+    Split s;
+    const cplx u00(c[0], c[1]), u01(c[2], c[3]), u10(c[4], c[5]), u11(c[6], c[7]);
+    if (c[1] == 0.0 && c[3] == 0.0 && c[5] == 0.0 && c[7] == 0.0 && c[0] == c[6] && c[2] == -c[4]) {
+        // a real rotation needs no phases; m keeps its sign
+        s.form_b = std::fabs(c[4]) > std::fabs(c[0]);
+        const double m = s.form_b ? c[4] : c[0];
+        if (m == 0.0) return Split{};
+        s.t = (s.form_b ? c[0] : c[4]) / m;
+        s.gm = m;
+    } else {
+        const double a = std::abs(u00), b = std::abs(u10);
+        cplx g;
+        if (a >= b) {
+            if (!(a > 0.0)) return Split{};
+            g = u00 / a;
+        } else {
+            g = a > 0.0 ? (u10 / b) * (-u01 / b) / (u11 / a) : u10 / b;
+            const double gn = std::abs(g);
+            if (!(gn > 0.0) || !std::isfinite(gn)) return Split{};
+            g /= gn;
+        }
+        if (b > 0.0) {
+            s.phi = u10 / (g * b);
+            s.lam = -u01 / (g * b);
+        } else {
+            s.lam = u11 / (g * a);
+        }
+        s.form_b = b > a;
+        const double m = s.form_b ? b : a;
+        s.t = (s.form_b ? a : b) / m;
+        s.gm = g * m;
+    }
+    cplx r00, r01, r10, r11;
+    if (!s.form_b) {
+        r00 = s.gm;
+        r01 = -s.gm * s.t * s.lam;
+        r10 = s.gm * s.t * s.phi;
+        r11 = s.gm * s.phi * s.lam;
+    } else {
+        r00 = s.gm * s.t;
+        r01 = -s.gm * s.lam;
+        r10 = s.gm * s.phi;
+        r11 = s.gm * s.t * s.phi * s.lam;
+    }
+    const double err = std::max(std::max(std::abs(r00 - u00), std::abs(r01 - u01)),
+                                std::max(std::abs(r10 - u10), std::abs(r11 - u11)));
+    s.ok = std::isfinite(err) && std::isfinite(s.t) && err <= 1e-15;
+    return s;
+}
+
+// A pending phase: exp(i theta) on the amplitudes whose bits in S (local bits and bits outside
+// the block, as global bits) have odd parity; v = exp(i theta).
+struct Pend {
+    uint32_t lmask, omask;
+    cplx v;
+};
+
+// What a plan's pass hands to the next: pending sets as global qubit masks, and the global phase.
+struct Carry {
+    std::vector<std::pair<uint32_t, cplx>> pend;
+    cplx g{1.0, 0.0};
+};
+
+constexpr int kMaxVariantBits = 5;      // pending sets one rotation may depend on at run time
+constexpr size_t kMaxAuxValues = 3000;  // constants per pass (kernel parameter space)
+
 const char* kPrelude = R"SRC(
 typedef unsigned int u32;
 typedef unsigned long long u64;
@@ -155,6 +246,11 @@ struct Gen {
     int phys[NR];
     uint32_t pm[R];  // local masks of the register bits in the current layout
     const char* T;
+    // deferred phases (compile-time bookkeeping; values go to the kernel's constant parameter)
+    std::vector<double> aux;
+    std::vector<Pend> pend;
+    cplx G{1.0, 0.0};
+    int uid = 0;
 
     std::string X(int i) const { return "x" + std::to_string(phys[i]); }
     std::string Y(int i) const { return "y" + std::to_string(phys[i]); }
@@ -344,12 +440,306 @@ struct Gen {
         os << "}\n";
     }
 
+    // ------------------------------------------------ deferred phases
+    int slot(double v) {
+        aux.push_back(v);
+        return (int)aux.size() - 1;
+    }
+    int slot2(cplx v) {
+        aux.push_back(v.real());
+        aux.push_back(v.imag());
+        return (int)aux.size() - 2;
+    }
+    static std::string av(int s) { return "A.v[" + std::to_string(s) + "]"; }
+    int local_of_reg(int M) const { return __builtin_ctz(pm[M]); }
+    uint32_t reg_part(uint32_t lmask) const {
+        uint32_t r, t;
+        split(lmask, r, t);
+        return r;
+    }
+    // run-time parity (an int expression, 0 or 1) of a set's thread bits and bits outside the
+    // block; "" when the set has none
+    std::string sel_expr(uint32_t lmask, uint32_t omask) const {
+        const uint32_t tb = lmask & ~regmask();
+        std::string e;
+        if (tb) e = "__popc(base & " + hexu(tb) + ")";
+        if (omask) e += std::string(e.empty() ? "" : " + ") + "__popc(outer & " + hexu(omask) + ")";
+        return e.empty() ? e : "((" + e + ") & 1)";
+    }
+    // one entry per set; an empty set has even parity and a phase of 1 is nothing
+    void normalize() {
+        std::vector<Pend> out;
+        for (const Pend& e : pend) {
+            bool merged = false;
+            for (Pend& o : out)
+                if (o.lmask == e.lmask && o.omask == e.omask) {
+                    o.v *= e.v;
+                    merged = true;
+                    break;
+                }
+            if (!merged) out.push_back(e);
+        }
+        pend.clear();
+        for (const Pend& e : out)
+            if ((e.lmask || e.omask) && !(e.v == cplx(1.0, 0.0))) pend.push_back(e);
+    }
+    bool holds(int q) const {
+        for (const Pend& e : pend)
+            if ((e.lmask >> q) & 1u) return true;
+        return false;
+    }
+    // distinct sets that remain of the pending sets holding q once q leaves them
+    int dep_count(int q) const {
+        std::vector<std::pair<uint32_t, uint32_t>> sets;
+        for (const Pend& e : pend) {
+            if (!((e.lmask >> q) & 1u)) continue;
+            const std::pair<uint32_t, uint32_t> r(e.lmask & ~(1u << q), e.omask);
+            if ((r.first || r.second) && std::find(sets.begin(), sets.end(), r) == sets.end()) sets.push_back(r);
+        }
+        return (int)sets.size();
+    }
+    void cmul_var(const std::string& v, const std::string& pr, const std::string& pi) {
+        os << "{ const " << T << " vr = " << v << "r, vi = " << v << "i; " << v << "r = " << pr << " * vr - (" << pi
+           << ") * vi; " << v << "i = " << pr << " * vi + (" << pi << ") * vr; }\n";
+    }
+
+    // The phase that the amplitudes with local bit q set take from the pending sets holding q,
+    // times `extra`; q leaves those sets:
+    //     exp(i theta (b_q ^ p)) = [p ? e : 1] * [b_q ? (p ? conj e : e) : 1],  p = parity(S \ {q}).
+    // The variants over p are constants; the run-time part of p selects one.  Returns, per
+    // register pair (by its low register index), the class (0: one, 1: minus one, 2: variables).
+    struct PairPhase {
+        int cls = 0;
+        std::string re[NR], im[NR];
+    };
+    PairPhase take_phase(int q, cplx extra) {
+        PairPhase P;
+        cplx ls = extra;
+        std::vector<Pend> dep, keep;
+        for (const Pend& e : pend) {
+            if (!((e.lmask >> q) & 1u)) {
+                keep.push_back(e);
+                continue;
+            }
+            const Pend r{e.lmask & ~(1u << q), e.omask, e.v};
+            if (!r.lmask && !r.omask) {
+                ls *= e.v;
+                continue;
+            }
+            bool merged = false;
+            for (Pend& d : dep)
+                if (d.lmask == r.lmask && d.omask == r.omask) {
+                    d.v *= r.v;
+                    merged = true;
+                }
+            if (!merged) dep.push_back(r);
+            keep.push_back(r);
+        }
+        pend.swap(keep);
+        normalize();
+        if (dep.empty()) {
+            if (ls == cplx(1.0, 0.0)) return P;
+            if (ls == cplx(-1.0, 0.0)) {
+                P.cls = 1;
+                return P;
+            }
+            const int s = slot2(ls);
+            const std::string n = "l" + std::to_string(uid++);
+            os << "const " << T << " " << n << "r = " << av(s) << ", " << n << "i = " << av(s + 1) << ";\n";
+            P.cls = 2;
+            for (int i = 0; i < NR; ++i) {
+                P.re[i] = n + "r";
+                P.im[i] = n + "i";
+            }
+            return P;
+        }
+        const int J = (int)dep.size();
+        const int first = (int)aux.size();
+        for (int key = 0; key < (1 << J); ++key) {
+            cplx v = ls;
+            for (int d = 0; d < J; ++d) v *= ((key >> d) & 1) ? std::conj(dep[d].v) : dep[d].v;
+            slot2(v);
+        }
+        std::string kr;
+        for (int d = 0; d < J; ++d) {
+            const std::string e = sel_expr(dep[d].lmask, dep[d].omask);
+            if (!e.empty()) kr += (kr.empty() ? "(" : " | (") + e + " << " + std::to_string(d) + ")";
+        }
+        const std::string id = std::to_string(uid++);
+        if (!kr.empty()) os << "const int k" << id << " = " << kr << ";\n";
+        P.cls = 2;
+        std::string declared[1 << kMaxVariantBits];
+        for (int i = 0; i < NR; ++i) {
+            int rk = 0;
+            for (int d = 0; d < J; ++d)
+                if (__builtin_popcount((uint32_t)i & reg_part(dep[d].lmask)) & 1) rk |= 1 << d;
+            if (declared[rk].empty()) {
+                const std::string n = "l" + id + "_" + std::to_string(rk);
+                const std::string at = kr.empty() ? std::to_string(first + 2 * rk)
+                                                  : std::to_string(first) + " + 2 * (k" + id + " ^ " + std::to_string(rk) + ")";
+                os << "const " << T << " " << n << "r = A.v[" << at << "], " << n << "i = A.v[" << at << " + 1];\n";
+                declared[rk] = n;
+            }
+            P.re[i] = declared[rk] + "r";
+            P.im[i] = declared[rk] + "i";
+        }
+        return P;
+    }
+    // Applies the pending phases that hold the qubit of register bit M (before an op on it that
+    // does not take them).
+    void resolve(int M) {
+        const int q = local_of_reg(M);
+        if (!holds(q)) return;
+        if (dep_count(q) > kMaxVariantBits) {
+            flush_all();
+            return;
+        }
+        os << "{\n";
+        const PairPhase P = take_phase(q, cplx(1.0, 0.0));
+        for (int i = 0; i < NR; ++i) {
+            if ((i >> M) & 1) continue;
+            const int k = i | (1 << M);
+            if (P.cls == 1) negate_reg(k);
+            else if (P.cls == 2) cmul_reg(k, P.re[i].c_str(), P.im[i].c_str());
+        }
+        os << "}\n";
+    }
+    // Multiplies every amplitude by its pending phase and by G; nothing is pending afterwards.
+    //     F(i) = G * prod_j ((par_j(i) ^ sel_j) ? e_j : 1)
+    // with par_j the parity of set j's register bits in register index i and sel_j that of its
+    // thread and outer bits.  The factors of sets without register bits multiply the thread
+    // factor; the others group by register mask m into q_m, and a Gray-code walk over the
+    // register indices steps F from one index to the next with one q_m (or its conjugate) per
+    // mask holding the flipped bit.
+    void flush_all() {
+        normalize();
+        if (pend.empty() && G == cplx(1.0, 0.0)) return;
+        const std::string f = "f" + std::to_string(uid++);
+        os << "{\n";
+        std::vector<uint32_t> masks;
+        std::vector<cplx> qc;
+        struct Rt {
+            std::string sel;
+            cplx v;
+            int group;
+        };
+        std::vector<Rt> rt;
+        for (const Pend& e : pend) {
+            const uint32_t rm = reg_part(e.lmask);
+            int gi = -1;
+            if (rm) {
+                for (size_t j = 0; j < masks.size(); ++j)
+                    if (masks[j] == rm) gi = (int)j;
+                if (gi < 0) {
+                    masks.push_back(rm);
+                    qc.push_back(cplx(1.0, 0.0));
+                    gi = (int)masks.size() - 1;
+                }
+            }
+            const std::string sel = sel_expr(e.lmask, e.omask);
+            if (sel.empty()) qc[(size_t)gi] *= e.v;
+            else rt.push_back({sel, e.v, gi});
+        }
+        const int gs = slot2(G);
+        os << T << " " << f << "r = " << av(gs) << ", " << f << "i = " << av(gs + 1) << ";\n";
+        std::vector<std::string> qn(masks.size());
+        std::vector<bool> qrun(masks.size(), false);
+        for (const Rt& r : rt)
+            if (r.group >= 0) qrun[(size_t)r.group] = true;
+        for (size_t j = 0; j < masks.size(); ++j) {
+            qn[j] = f + "q" + std::to_string(j);
+            const int s = slot2(qc[j]);
+            os << (qrun[j] ? "" : "const ") << T << " " << qn[j] << "r = " << av(s) << ", " << qn[j]
+               << "i = " << av(s + 1) << ";\n";
+        }
+        for (const Rt& r : rt) {
+            const int s = slot2(r.v);
+            os << "{ const bool s = " << r.sel << " != 0;\n";
+            os << "const " << T << " er = s ? " << av(s) << " : (" << T << ")1, ei = s ? " << av(s + 1) << " : (" << T
+               << ")0;\n";
+            cmul_var(f, "er", "ei");
+            if (r.group >= 0) {
+                os << "const " << T << " qr = " << av(s) << ", qi = s ? -" << av(s + 1) << " : " << av(s + 1) << ";\n";
+                cmul_var(qn[(size_t)r.group], "qr", "qi");
+            }
+            os << "}\n";
+        }
+        cmul_reg(0, (f + "r").c_str(), (f + "i").c_str());
+        for (int k = 1; k < NR; ++k) {
+            const int prev = (k - 1) ^ ((k - 1) >> 1), cur = k ^ (k >> 1);
+            const int b = __builtin_ctz((unsigned)k);
+            for (size_t j = 0; j < masks.size(); ++j) {
+                if (!((masks[j] >> b) & 1u)) continue;
+                // entering odd parity takes q_m, leaving it takes conj(q_m)
+                const bool odd = __builtin_popcount((uint32_t)prev & masks[j]) & 1;
+                cmul_var(f, qn[j] + "r", (odd ? "-" : "") + qn[j] + "i");
+            }
+            cmul_reg(cur, (f + "r").c_str(), (f + "i").c_str());
+        }
+        os << "}\n";
+        pend.clear();
+        G = cplx(1.0, 0.0);
+    }
+    // Multiplies by |G| so that magnitudes stay those of the state; G keeps its phase.
+    void rescale() {
+        const double r = std::abs(G);
+        if (r == 1.0) return;
+        const int s = slot(r);
+        os << "{ const " << T << " r = " << av(s) << ";\n";
+        for (int i = 0; i < NR; ++i) os << X(i) << " *= r; " << Y(i) << " *= r;\n";
+        os << "}\n";
+        G /= r;
+    }
+    bool rotatable(const FusedOp& op) const {
+        return (op.code == OP_MATRIX || op.code == OP_MATRIX_REAL) && !(op.flags & (kOpTable | kOpBranch)) &&
+               op.cmask_local == 0 && op.cmask_outer == 0 && aux.size() < kMaxAuxValues;
+    }
+    // An uncontrolled unitary on register bit M as a scaled rotation between two deferred phases.
+    void rotation(const FusedOp& op, const Split& sp) {
+        const int M = op.reg, q = local_of_reg(M);
+        if (dep_count(q) > kMaxVariantBits) flush_all();
+        os << "{\n";
+        const PairPhase P = take_phase(q, sp.lam);
+        const int ts = slot(sp.t);
+        os << "const " << T << " t = " << av(ts) << ";\n";
+        for (int i = 0; i < NR; ++i) {
+            if ((i >> M) & 1) continue;
+            const int k = i | (1 << M);
+            os << "{ const " << T << " xr = " << X(i) << ", xi = " << Y(i) << ";\n";
+            if (P.cls == 0)
+                os << "const " << T << " wr = " << X(k) << ", wi = " << Y(k) << ";\n";
+            else if (P.cls == 1)
+                os << "const " << T << " wr = -" << X(k) << ", wi = -" << Y(k) << ";\n";
+            else
+                os << "const " << T << " wr = " << P.re[i] << " * " << X(k) << " - " << P.im[i] << " * " << Y(k)
+                   << ", wi = " << P.re[i] << " * " << Y(k) << " + " << P.im[i] << " * " << X(k) << ";\n";
+            if (!sp.form_b)
+                os << X(i) << " = xr - t * wr; " << Y(i) << " = xi - t * wi; " << X(k) << " = t * xr + wr; " << Y(k)
+                   << " = t * xi + wi; }\n";
+            else
+                os << X(i) << " = t * xr - wr; " << Y(i) << " = t * xi - wi; " << X(k) << " = xr + t * wr; " << Y(k)
+                   << " = xi + t * wi; }\n";
+        }
+        os << "}\n";
+        if (!(sp.phi == cplx(1.0, 0.0))) pend.push_back({1u << q, 0u, sp.phi});
+        normalize();
+        G *= sp.gm;
+    }
+
     void op(int o, const FusedOp& op) {
         uint32_t rm, tb;
         split(op.cmask_local, rm, tb);
         switch (op.code) {
         case OP_MATRIX:
         case OP_MATRIX_REAL: {
+            if (rotatable(op)) {
+                const Split sp = split_unitary(op.coef);
+                if (sp.ok) {
+                    rotation(op, sp);
+                    break;
+                }
+            }
+            resolve(op.reg);
             const int M = op.reg;
             const int n = open_conditions(op.cmask_outer, tb);
             const std::string c = coef_ptr(o, op);
@@ -381,6 +771,25 @@ struct Gen {
         }
         case OP_EXCHANGE: {
             const int M = op.reg;
+            // X: parity p -> p ^ 1, so exp(i theta p) = e * conj(e)^p; one control c: S ^= {c}
+            const int q = local_of_reg(M);
+            const int nc = __builtin_popcount(op.cmask_local) + __builtin_popcount(op.cmask_outer);
+            if (nc == 0) {
+                for (Pend& e : pend)
+                    if ((e.lmask >> q) & 1u) {
+                        G *= e.v;
+                        e.v = std::conj(e.v);
+                    }
+            } else if (nc == 1) {
+                for (Pend& e : pend)
+                    if ((e.lmask >> q) & 1u) {
+                        e.lmask ^= op.cmask_local;
+                        e.omask ^= op.cmask_outer;
+                    }
+                normalize();
+            } else {
+                resolve(M);
+            }
             std::vector<std::pair<int, int>> prs;
             for (int i = 0; i < NR; ++i)
                 if (!((i >> M) & 1) && ((uint32_t)i & rm) == rm) prs.push_back({i, i | (1 << M)});
@@ -392,6 +801,15 @@ struct Gen {
         }
         case OP_SWAP: {
             const int M1 = op.reg, M2 = op.reg2;
+            if (op.cmask_local == 0 && op.cmask_outer == 0) {
+                const uint32_t b1 = 1u << local_of_reg(M1), b2 = 1u << local_of_reg(M2);
+                for (Pend& e : pend)
+                    if (((e.lmask & b1) != 0) != ((e.lmask & b2) != 0)) e.lmask ^= b1 | b2;
+                normalize();
+            } else {
+                resolve(M1);
+                resolve(M2);
+            }
             std::vector<std::pair<int, int>> prs;
             for (int i = 0; i < NR; ++i)
                 if (((i >> M1) & 1) && !((i >> M2) & 1) && ((uint32_t)i & rm) == rm)
@@ -409,14 +827,32 @@ struct Gen {
     }
 };
 
-// The whole source of one pass's kernel; structurally equal passes give the same text.
-std::string generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, bool fp64) {
+// The source of one pass's kernel and the constants it takes (kernel parameter `A`).  The source
+// depends on the pass structure and on which form each rotation takes, never on the angles.
+// With `carry`, pending phases come in from the previous pass and, unless `last`, go on to the
+// next one; without it the pass is self-contained.
+struct Generated {
+    std::string src;
+    std::vector<unsigned char> aux;  // the parameter block: doubles (complex128) or floats
+};
+
+Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, bool fp64, Carry* carry, bool last) {
     Gen g;
     g.fp64 = fp64;
     g.K = p.k;
     g.T = fp64 ? "double" : "float";
     for (int i = 0; i < NR; ++i) g.phys[i] = i;
     g.set_layout(p.reg_in);
+    if (carry) {
+        for (const auto& e : carry->pend) {
+            Pend x{0u, e.first & ~p.block_mask, e.second};
+            for (int b = 0; b < p.k; ++b)
+                if (e.first & (1u << p.q[b])) x.lmask |= 1u << b;
+            g.pend.push_back(x);
+        }
+        g.G = carry->g;
+        g.normalize();
+    }
     uint32_t thread_in = 0, thread_out = 0, reg_in_local = 0, reg_out_local = 0;
     uint32_t reg_in_g[R], reg_out_g[R];
     for (int m = 0; m < R; ++m) {
@@ -430,25 +866,15 @@ std::string generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, b
         if (!(reg_out_local & (1u << b))) thread_out |= 1u << p.q[b];
     }
     const int nt = 1 << (p.k - R);
-    // 128 registers per thread: two 256-thread blocks per SM (complex128, 12 qubits), one
-    // 512-thread block (complex64, 13 qubits); fewer would spill the 16 amplitudes
-    const int minb = (fp64 && p.k == 12) ? 2 : 1;
+    // 128 registers per thread, so 512 threads per SM in as many blocks as that makes (two
+    // blocks of 12 qubits, four of 11); fewer registers would spill the 16 amplitudes
+    const int minb = p.k >= 13 ? 1 : 1 << (13 - p.k);
     const size_t tile_bytes = (size_t)(fp64 ? 16 : 8) << p.k;
     const size_t prog_bytes = ((size_t)p.op_count * sizeof(FusedOp) + 15) & ~size_t(15);
     bool tabled = false;
     for (int o = 0; o < p.op_count; ++o)
         if (plan_ops[(size_t)(p.op_begin + o)].flags & kOpTable) tabled = true;
-    std::ostringstream& os = g.os;
-    os << kPrelude;
-    os << "typedef " << (fp64 ? "double2" : "float2") << " V;\n";
-    if (fp64)
-        os << "__device__ __forceinline__ u32 qm_swz(u32 j) { const u32 h = j >> 3; return j ^ ((h ^ (h >> 3) ^ (h >> 6) "
-              "^ (h >> 9)) & 7u); }\n";
-    else
-        os << "__device__ __forceinline__ u32 qm_swz(u32 j) { const u32 h = j >> 4; return j ^ ((h ^ (h >> 4) ^ (h >> 8)) "
-              "& 15u); }\n";
-    os << "extern \"C\" __global__ void __launch_bounds__(" << nt << ", " << minb
-       << ") qm_pass(V* __restrict__ s0, const __grid_constant__ FusedLaunch P) {\n";
+    std::ostringstream& os = g.os;  // the kernel body
     os << "extern __shared__ __align__(16) unsigned char smem_raw[];\n";
     os << "V* tile = reinterpret_cast<V*>(smem_raw);\n";
     os << "FusedOp* prog = reinterpret_cast<FusedOp*>(smem_raw + " << tile_bytes << ");\n";
@@ -495,6 +921,24 @@ std::string generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, b
         }
         g.op(o, op);
     }
+    if (carry && !last) {
+        g.rescale();
+        g.normalize();
+        carry->pend.clear();
+        for (const Pend& e : g.pend) {
+            uint32_t gm = e.omask;
+            for (int b = 0; b < p.k; ++b)
+                if (e.lmask & (1u << b)) gm |= 1u << p.q[b];
+            carry->pend.push_back({gm, e.v});
+        }
+        carry->g = g.G;
+    } else {
+        g.flush_all();
+        if (carry) {
+            carry->pend.clear();
+            carry->g = cplx(1.0, 0.0);
+        }
+    }
     os << "{ const u32 g1 = outer | " << deposit_expr("t", thread_out) << ";\n";
     for (int i = 0; i < NR; ++i) {
         uint32_t gi = 0;
@@ -503,7 +947,48 @@ std::string generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, b
         os << "{ V v; v.x = " << g.X(i) << "; v.y = " << g.Y(i) << "; s[g1 | " << hexu(gi) << "] = v; }\n";
     }
     os << "}\n(void)base;\n}\n}\n";
-    return os.str();
+
+    std::ostringstream hd;
+    hd << kPrelude;
+    hd << "typedef " << (fp64 ? "double2" : "float2") << " V;\n";
+    if (fp64)
+        hd << "__device__ __forceinline__ u32 qm_swz(u32 j) { const u32 h = j >> 3; return j ^ ((h ^ (h >> 3) ^ (h >> 6) "
+              "^ (h >> 9)) & 7u); }\n";
+    else
+        hd << "__device__ __forceinline__ u32 qm_swz(u32 j) { const u32 h = j >> 4; return j ^ ((h ^ (h >> 4) ^ (h >> 8)) "
+              "& 15u); }\n";
+    const size_t na = std::max<size_t>(1, g.aux.size());
+    hd << "struct Aux { " << g.T << " v[" << na << "]; };\n";
+    hd << "extern \"C\" __global__ void __launch_bounds__(" << nt << ", " << minb
+       << ") qm_pass(V* __restrict__ s0, const __grid_constant__ FusedLaunch P, const __grid_constant__ Aux A) {\n";
+    Generated out;
+    // the constants travel as a kernel parameter (at most 32764 bytes with the launch record)
+    if (g.aux.size() > kMaxAuxValues + 1000) return out;
+    out.src = hd.str() + os.str();
+    if (fp64) {
+        std::vector<double> v(na, 0.0);
+        std::copy(g.aux.begin(), g.aux.end(), v.begin());
+        out.aux.resize(na * sizeof(double));
+        std::memcpy(out.aux.data(), v.data(), out.aux.size());
+    } else {
+        std::vector<float> v(na, 0.0f);
+        for (size_t i = 0; i < g.aux.size(); ++i) v[i] = (float)g.aux[i];
+        out.aux.resize(na * sizeof(float));
+        std::memcpy(out.aux.data(), v.data(), out.aux.size());
+    }
+    return out;
+}
+
+// Every pass of a plan: chained (phases carried from pass to pass, flushed by the last) or
+// self-contained.
+std::vector<Generated> generate_plan(const Plan& plan, bool chained) {
+    const bool fp64 = plan.precision != QM_FP32;
+    std::vector<Generated> out;
+    out.reserve(plan.passes.size());
+    Carry carry;
+    for (size_t i = 0; i < plan.passes.size(); ++i)
+        out.push_back(generate(plan.passes[i], plan.ops, fp64, chained ? &carry : nullptr, i + 1 == plan.passes.size()));
+    return out;
 }
 
 // ---------------------------------------------------------------- compiled-kernel cache
@@ -551,6 +1036,7 @@ cudaKernel_t compile_source(const std::string& src) {
 }
 
 cudaKernel_t kernel_for(const std::string& src) {
+    if (src.empty()) return nullptr;  // a pass whose constants do not fit a kernel parameter
     {
         std::lock_guard<std::mutex> lock(g_cache_mu);
         auto it = g_cache.find(src);
@@ -571,18 +1057,15 @@ bool jit_enabled() { return kRegBits == 4 && nvrtc().ok; }
 
 }  // namespace
 
-void jit_prepare(Plan& plan) {
-    plan.jit.assign(plan.passes.size(), nullptr);
-    if (!jit_enabled() || plan.passes.empty()) return;
-    const bool fp64 = plan.precision != QM_FP32;
-    std::vector<std::string> src(plan.passes.size());
-    for (size_t i = 0; i < plan.passes.size(); ++i) src[i] = generate(plan.passes[i], plan.ops, fp64);
-    // compile the distinct sources in parallel
+namespace {
+
+// Compiles the distinct sources in parallel; returns whether every one compiled.
+bool compile_all(const std::vector<Generated>& gen) {
     std::vector<size_t> todo;
     {
         std::unordered_map<std::string, size_t> first;
-        for (size_t i = 0; i < src.size(); ++i)
-            if (first.emplace(src[i], i).second) todo.push_back(i);
+        for (size_t i = 0; i < gen.size(); ++i)
+            if (first.emplace(gen[i].src, i).second) todo.push_back(i);
     }
     int device = 0;
     cudaGetDevice(&device);
@@ -592,30 +1075,80 @@ void jit_prepare(Plan& plan) {
     for (size_t w = 0; w < workers; ++w)
         pool.emplace_back([&]() {
             cudaSetDevice(device);
-            for (size_t j; (j = next.fetch_add(1)) < todo.size();) kernel_for(src[todo[j]]);
+            for (size_t j; (j = next.fetch_add(1)) < todo.size();) kernel_for(gen[todo[j]].src);
         });
     for (auto& th : pool) th.join();
-    for (size_t i = 0; i < src.size(); ++i) plan.jit[i] = reinterpret_cast<const void*>(kernel_for(src[i]));
+    bool all = true;
+    for (const Generated& g : gen)
+        if (!kernel_for(g.src)) all = false;
+    return all;
+}
+
+void install(Plan& plan, std::vector<Generated>& gen, bool cached_only) {
+    for (size_t i = 0; i < gen.size(); ++i) {
+        const void* k = nullptr;
+        if (cached_only) {
+            std::lock_guard<std::mutex> lock(g_cache_mu);
+            auto it = g_cache.find(gen[i].src);
+            if (it != g_cache.end() && !it->second.failed) k = reinterpret_cast<const void*>(it->second.kernel);
+        } else {
+            k = reinterpret_cast<const void*>(kernel_for(gen[i].src));
+        }
+        plan.jit[i] = k;
+        if (k) plan.jit_aux[i] = std::move(gen[i].aux);
+    }
+}
+
+bool all_cached(const std::vector<Generated>& gen) {
+    std::lock_guard<std::mutex> lock(g_cache_mu);
+    for (const Generated& g : gen) {
+        if (g.src.empty()) return false;
+        auto it = g_cache.find(g.src);
+        if (it == g_cache.end() || it->second.failed) return false;
+    }
+    return true;
+}
+
+}  // namespace
+
+// Chained passes need every pass compiled; otherwise each pass is made self-contained and those
+// that compile run compiled, the others on the interpreter.
+void jit_prepare(Plan& plan) {
+    plan.jit.assign(plan.passes.size(), nullptr);
+    plan.jit_aux.assign(plan.passes.size(), {});
+    if (!jit_enabled() || plan.passes.empty()) return;
+    std::vector<Generated> gen = generate_plan(plan, true);
+    if (compile_all(gen)) {
+        install(plan, gen, false);
+        return;
+    }
+    gen = generate_plan(plan, false);
+    compile_all(gen);
+    install(plan, gen, false);
 }
 
 void jit_lookup(Plan& plan) {
     plan.jit.assign(plan.passes.size(), nullptr);
+    plan.jit_aux.assign(plan.passes.size(), {});
     if (!jit_enabled() || plan.passes.empty()) return;
     {
         std::lock_guard<std::mutex> lock(g_cache_mu);
         if (g_cache.empty()) return;
     }
-    const bool fp64 = plan.precision != QM_FP32;
-    std::lock_guard<std::mutex> lock(g_cache_mu);
-    for (size_t i = 0; i < plan.passes.size(); ++i) {
-        auto it = g_cache.find(generate(plan.passes[i], plan.ops, fp64));
-        if (it != g_cache.end() && !it->second.failed) plan.jit[i] = reinterpret_cast<const void*>(it->second.kernel);
+    std::vector<Generated> gen = generate_plan(plan, true);
+    if (all_cached(gen)) {
+        install(plan, gen, true);
+        return;
     }
+    gen = generate_plan(plan, false);
+    install(plan, gen, true);
 }
 
 cudaError_t launch_plan_pass(const Plan& plan, size_t pass, void* amps, const FusedBatch* batch, cudaStream_t st) {
     const FusedPass& p = plan.passes[pass];
-    const void* kernel = pass < plan.jit.size() ? plan.jit[pass] : nullptr;
+    const void* kernel = pass < plan.jit.size() && pass < plan.jit_aux.size() && !plan.jit_aux[pass].empty()
+                             ? plan.jit[pass]
+                             : nullptr;
     if (!kernel) return launch_fused(amps, plan.qubits, plan.precision, p, plan.d_ops, batch, st);
     if (batch && (batch->states < 1 || batch->states > 65535)) return cudaErrorInvalidValue;
     FusedLaunch L = fused_launch_params(plan.qubits, p, plan.d_ops, batch);
@@ -637,7 +1170,7 @@ cudaError_t launch_plan_pass(const Plan& plan, size_t pass, void* amps, const Fu
     const int64_t items = (int64_t)L.states << L.cta_shift;
     const int64_t grid = std::min<int64_t>(items, (int64_t)sms * per_sm);
     void* arg0 = amps;
-    void* args[] = {&arg0, &L};
+    void* args[] = {&arg0, &L, const_cast<unsigned char*>(plan.jit_aux[pass].data())};
     e = cudaLaunchKernel(kernel, dim3((unsigned)grid), dim3((unsigned)threads), args, smem, st);
     if (e == cudaSuccess) ++g_launches;
     return e;
@@ -664,7 +1197,7 @@ extern "C" int32_t qm_jit_source(int32_t qubits, int32_t precision, const qm_gat
     std::vector<qm_gate> list(gates, gates + count);
     if (!plan_fused(list, qubits, precision, fusion_width, plan, err)) return fail(QM_E_ARG, "planner: " + err);
     if (pass < 0 || (size_t)pass >= plan.passes.size()) return fail(QM_E_RANGE, "pass index out of range");
-    const std::string src = generate(plan.passes[(size_t)pass], plan.ops, precision != QM_FP32);
+    const std::string src = generate_plan(plan, true)[(size_t)pass].src;
     if (length) *length = src.size();
     if (buffer && size) {
         const size_t n = std::min(size - 1, src.size());

@@ -8,6 +8,7 @@ Toffolis, X controls on thread bits and on qubits outside the block.
 from __future__ import annotations
 
 import ctypes as C
+import re
 
 import numpy as np
 import pytest
@@ -27,19 +28,42 @@ def jit_info():
     return avail.value, kernels.value, failed.value, launches.value
 
 
-def test_generated_source_is_structural():
-    """Sources depend on the pass structure, not on the angles."""
-    a, na = prepare(brick_circuit(14, 4, seed=1))
-    b, nb = prepare(brick_circuit(14, 4, seed=2))
+def perturbed_brick(n: int, depth: int, eps: float):
+    """The brick circuit's structure with every angle moved by eps."""
+    from quantummatter_b200.circuit import QuantumCircuit, u3
+    from quantummatter_b200.workloads import SplitMix64
+    rng, c = SplitMix64(1), QuantumCircuit(n)
+    for layer in range(depth):
+        for q in range(n):
+            th, ph, la = (rng.uniform(0, 2 * np.pi) + eps for _ in range(3))
+            c.U(q, u3(th, ph, la))
+        for q in range(layer % 2, n - 1, 2):
+            c.CNot(q, q + 1)
+    return c
+
+
+def jit_sources(c, passes):
+    g, n = prepare(c)
     out = []
-    for g, n in ((a, na), (b, nb)):
+    for p in passes:
         ln = C.c_size_t()
-        check(load().qm_jit_source(14, FP64, g, n, 0, 0, None, 0, C.byref(ln)))
+        check(load().qm_jit_source(c.QubitCount, FP64, g, n, 0, p, None, 0, C.byref(ln)))
         buf = C.create_string_buffer(ln.value + 1)
-        check(load().qm_jit_source(14, FP64, g, n, 0, 0, buf, ln.value + 1, C.byref(ln)))
+        check(load().qm_jit_source(c.QubitCount, FP64, g, n, 0, p, buf, ln.value + 1, C.byref(ln)))
         out.append(buf.value.decode())
-    assert out[0] == out[1]
-    assert "qm_pass" in out[0] and "prog[" in out[0]
+    return out
+
+
+def test_generated_source_is_structural():
+    """Sources hold the pass structure and the form of each rotation; the angles and every
+    constant derived from them travel in the kernel's parameter block."""
+    a = jit_sources(perturbed_brick(14, 4, 0.0), [0, 1])
+    b = jit_sources(perturbed_brick(14, 4, 1e-9), [0, 1])
+    assert a == b
+    assert "qm_pass" in a[0] and "A.v[" in a[0] and "__grid_constant__ Aux A" in a[0]
+    # the first pass rescales and carries its pending phases; the last multiplies them in
+    assert re.search(r"const double r = A\.v\[", a[0]) and not re.search(r"\bf\d+r = A\.v\[", a[0])
+    assert re.search(r"\bf\d+r = A\.v\[", a[1])
 
 
 @pytest.mark.gpu
