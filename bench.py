@@ -640,7 +640,7 @@ def main() -> None:
 def plan_width(passes: int, qubits: int, precision: int, width: int) -> int:
     if width:
         return width
-    return min(13 if precision == 1 else 12, qubits)
+    return min(12, qubits)
 
 
 if __name__ == "__main__":
