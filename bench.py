@@ -573,8 +573,9 @@ def main() -> None:
         if passes else f"k_gate_{args.precision}_{qubits}q"
     traffic = profile_traffic(kernel_key)
 
-    # FP64/FP32 arithmetic of the dense 2x2 gates (H, Rx, Ry, Unitary): 16 real flops per amplitude;
-    # permutations and diagonal phases are counted as free
+    # arithmetic a dense 2x2 product would issue for the H, Rx, Ry and Unitary gates (16 real flops
+    # per amplitude; permutations and diagonal phases free).  The compiled passes issue 8 per
+    # amplitude for a general unitary (a scaled rotation between deferred phases), 4 for a real one.
     dense = sum(1 for op in circuit.Operations if int(op.Kind) in (0, 6, 7, 15))
     flops = dense * amps * 8 * 2
     e2e = None
@@ -617,7 +618,7 @@ def main() -> None:
                          "frac": achieved_gbs / hbm_peak, "traffic": traffic, "peak_source": peak_kind,
                          "kernel": kernel_key, "algorithmic_bytes_per_launch": bytes_per_launch,
                          "launch_ms": 1e3 * per_launch_s,
-                         "fp_alu_tflops": flops * args.steps / total / 1e12},
+                         "dense_2x2_equivalent_tflops": flops * args.steps / total / 1e12},
             "gpu_launches": args.steps * launches,
             "clocks": clocks.summary(),
             "wall_s_timed": wall,
