@@ -110,6 +110,7 @@ struct Plan {
     FusedOp* d_ops = nullptr;       // device copy of ops (each pass's program is staged from it)
     std::vector<const void*> jit;   // per pass: compiled kernel (cudaKernel_t) or null
     std::vector<std::vector<unsigned char>> jit_aux;  // per pass: the compiled kernel's constants
+    std::vector<int> jit_tiles;     // per pass: shared-memory tiles of the compiled kernel (2: pipelined)
     bool borrowed = false;          // d_ops belongs to a context buffer
     int64_t planned_bytes = 0;
     int32_t launches = 0;

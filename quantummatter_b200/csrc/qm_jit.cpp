@@ -834,9 +834,11 @@ struct Gen {
 struct Generated {
     std::string src;
     std::vector<unsigned char> aux;  // the parameter block: doubles (complex128) or floats
+    int tiles = 1;                   // tiles of shared memory (2: pipelined)
 };
 
-Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, bool fp64, Carry* carry, bool last) {
+Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int qubits, bool fp64, Carry* carry,
+                   bool last) {
     Gen g;
     g.fp64 = fp64;
     g.K = p.k;
@@ -866,28 +868,66 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, boo
         if (!(reg_out_local & (1u << b))) thread_out |= 1u << p.q[b];
     }
     const int nt = 1 << (p.k - R);
-    // 128 registers per thread, so 512 threads per SM in as many blocks as that makes (two
-    // blocks of 12 qubits, four of 11); fewer registers would spill the 16 amplitudes
-    const int minb = p.k >= 13 ? 1 : 1 << (13 - p.k);
     const size_t tile_bytes = (size_t)(fp64 ? 16 : 8) << p.k;
     const size_t prog_bytes = ((size_t)p.op_count * sizeof(FusedOp) + 15) & ~size_t(15);
     bool tabled = false;
     for (int o = 0; o < p.op_count; ++o)
         if (plan_ops[(size_t)(p.op_begin + o)].flags & kOpTable) tabled = true;
+    // The tile pipeline needs a second tile of shared memory.  Complex64 blocks of 12 qubits keep
+    // two blocks per SM with it (5.9 against 6.5 ms per 30-qubit brick pass).  A complex128 block
+    // would take an SM alone, and one 8-warp block per SM computes too slowly (12.3 against
+    // 10.7 ms).  States of fewer than 26 qubits largely stay in L2, where the extra trip through
+    // shared memory costs more than it hides, and passes with a batch table lose more from
+    // reading it without staging: all of those load straight from global memory.
+    const bool piped = !fp64 && !tabled && qubits >= 26 && 2 * tile_bytes + prog_bytes <= (100u << 10);
+    const int tiles = piped ? 2 : 1;
+    // Blocks per SM: 128 registers per thread (512 threads per SM; fewer registers would spill
+    // the 16 amplitudes) and the shared memory (a pipelined complex128 block of 12 qubits takes
+    // an SM alone).
+    const int minb =
+        std::max(1, std::min(512 / nt, (int)((220u << 10) / (tiles * tile_bytes + prog_bytes + 8192))));
     std::ostringstream& os = g.os;  // the kernel body
     os << "extern __shared__ __align__(16) unsigned char smem_raw[];\n";
     os << "V* tile = reinterpret_cast<V*>(smem_raw);\n";
-    os << "FusedOp* prog = reinterpret_cast<FusedOp*>(smem_raw + " << tile_bytes << ");\n";
-    os << "double* table = reinterpret_cast<double*>(smem_raw + " << (tile_bytes + prog_bytes) << ");\n";
+    if (piped) os << "V* ptile = reinterpret_cast<V*>(smem_raw + " << tile_bytes << ");\n";
+    os << "FusedOp* prog = reinterpret_cast<FusedOp*>(smem_raw + " << tiles * tile_bytes << ");\n";
+    os << "double* table = reinterpret_cast<double*>(smem_raw + " << (tiles * tile_bytes + prog_bytes) << ");\n";
     os << "const u32 t = threadIdx.x;\n";
     os << "{ const uint2* src = reinterpret_cast<const uint2*>(P.ops); uint2* dst = reinterpret_cast<uint2*>(prog);\n"
        << "  for (int i = t; i < " << p.op_count * (int)(sizeof(FusedOp) / 8) << "; i += " << nt
        << ") dst[i] = __ldg(src + i); }\n";
     os << "const long long total = (long long)P.states << P.cta_shift;\n";
     os << "const u32 cta_mask = (1u << P.cta_shift) - 1u;\n";
+    // Tile pipeline: the next work item's tile is copied into `ptile` (cp.async, no registers)
+    // while this one computes.  Thread t copies local indices t + nt*r, r < 16: consecutive
+    // threads take consecutive amplitudes, so the copies come in the block's 128-byte runs.
+    if (piped) {
+        uint32_t lo = 0;
+        for (int b = 0; b < p.k - R; ++b) lo |= 1u << p.q[b];
+        os << "const u32 pf_g = " << deposit_expr("t", lo) << ";\n";
+        os << "const u32 pf_b = (u32)__cvta_generic_to_shared(ptile), pf_w = qm_swz(t);\n";
+    }
+    auto prefetch = [&](const char* item_expr) {
+        if (!piped) return;
+        os << "{ const long long it = " << item_expr << ";\nif (it < total) {\n"
+           << "const V* src = s0 + (u64)(int)(it >> P.cta_shift) * P.state_stride + (qm_deposit((u32)it & cta_mask, P.outer_mask) | pf_g);\n";
+        for (int r = 0; r < NR; ++r) {
+            uint32_t hi = 0;
+            for (int m = 0; m < R; ++m)
+                if ((r >> m) & 1) hi |= 1u << p.q[p.k - R + m];
+            // slot of local index t + nt*r: the swizzle is linear, so qm_swz(t) ^ qm_swz(nt*r)
+            os << "asm volatile(\"cp.async." << (fp64 ? "cg" : "ca") << ".shared.global [%0], [%1], " << (fp64 ? 16 : 8)
+               << ";\" :: \"r\"(pf_b + ((pf_w ^ " << hexu(swz_host((uint32_t)(nt * r), fp64)) << ") << " << (fp64 ? 4 : 3)
+               << ")), \"l\"(src + " << hexu(hi) << ") : \"memory\");\n";
+        }
+        os << "}\nasm volatile(\"cp.async.commit_group;\" ::: \"memory\"); }\n";
+    };
+    prefetch("(long long)blockIdx.x");
     os << "int current = -1;\n";
     os << "for (long long item = blockIdx.x; item < total; item += gridDim.x) {\n";
-    os << "const int b = (int)(item >> P.cta_shift);\nconst u32 cta = (u32)item & cta_mask;\n__syncthreads();\n";
+    os << "const int b = (int)(item >> P.cta_shift);\nconst u32 cta = (u32)item & cta_mask;\n";
+    if (piped) os << "asm volatile(\"cp.async.wait_group 0;\" ::: \"memory\");\n";
+    os << "__syncthreads();\n";
     if (tabled)
         os << "if (P.table_slots > 0 && b != current) { const double* row = P.table + (u64)b * P.table_stride;\n"
            << "  for (int i = t; i < 8 * P.table_slots; i += " << nt << ") table[i] = __ldg(row + i); __syncthreads(); }\n";
@@ -898,15 +938,24 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, boo
     for (int i = 1; i < NR; ++i) os << ", x" << i;
     for (int i = 0; i < NR; ++i) os << ", y" << i;
     os << ";\n";
-    os << "{ const u32 g0 = outer | " << deposit_expr("t", thread_in) << ";\n";
-    for (int i = 0; i < NR; ++i) {
-        uint32_t gi = 0;
-        for (int m = 0; m < R; ++m)
-            if ((i >> m) & 1) gi |= reg_in_g[m];
-        os << "{ const V v = s[g0 | " << hexu(gi) << "]; x" << i << " = v.x; y" << i << " = v.y; }\n";
+    if (piped) {
+        os << "u32 base = " << g.base_expr() << ";\n";
+        os << "{ const u32 sn = qm_swz(base);\n";
+        for (int i = 0; i < NR; ++i)
+            os << "{ const V v = ptile[sn ^ " << hexu(g.const_slot(i)) << "]; x" << i << " = v.x; y" << i << " = v.y; }\n";
+        os << "}\n__syncthreads();\n";
+        prefetch("item + gridDim.x");
+    } else {
+        os << "{ const u32 g0 = outer | " << deposit_expr("t", thread_in) << ";\n";
+        for (int i = 0; i < NR; ++i) {
+            uint32_t gi = 0;
+            for (int m = 0; m < R; ++m)
+                if ((i >> m) & 1) gi |= reg_in_g[m];
+            os << "{ const V v = s[g0 | " << hexu(gi) << "]; x" << i << " = v.x; y" << i << " = v.y; }\n";
+        }
+        os << "}\n";
+        os << "u32 base = " << g.base_expr() << ";\n";
     }
-    os << "}\n";
-    os << "u32 base = " << g.base_expr() << ";\n";
     for (int o = 0; o < p.op_count; ++o) {
         const FusedOp& op = plan_ops[(size_t)(p.op_begin + o)];
         if (op.code == OP_STAGE) {
@@ -965,6 +1014,7 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, boo
     // the constants travel as a kernel parameter (at most 32764 bytes with the launch record)
     if (g.aux.size() > kMaxAuxValues + 1000) return out;
     out.src = hd.str() + os.str();
+    out.tiles = tiles;
     if (fp64) {
         std::vector<double> v(na, 0.0);
         std::copy(g.aux.begin(), g.aux.end(), v.begin());
@@ -987,7 +1037,8 @@ std::vector<Generated> generate_plan(const Plan& plan, bool chained) {
     out.reserve(plan.passes.size());
     Carry carry;
     for (size_t i = 0; i < plan.passes.size(); ++i)
-        out.push_back(generate(plan.passes[i], plan.ops, fp64, chained ? &carry : nullptr, i + 1 == plan.passes.size()));
+        out.push_back(generate(plan.passes[i], plan.ops, plan.qubits, fp64, chained ? &carry : nullptr,
+                               i + 1 == plan.passes.size()));
     return out;
 }
 
@@ -1095,7 +1146,10 @@ void install(Plan& plan, std::vector<Generated>& gen, bool cached_only) {
             k = reinterpret_cast<const void*>(kernel_for(gen[i].src));
         }
         plan.jit[i] = k;
-        if (k) plan.jit_aux[i] = std::move(gen[i].aux);
+        if (k) {
+            plan.jit_aux[i] = std::move(gen[i].aux);
+            plan.jit_tiles[i] = gen[i].tiles;
+        }
     }
 }
 
@@ -1116,6 +1170,7 @@ bool all_cached(const std::vector<Generated>& gen) {
 void jit_prepare(Plan& plan) {
     plan.jit.assign(plan.passes.size(), nullptr);
     plan.jit_aux.assign(plan.passes.size(), {});
+    plan.jit_tiles.assign(plan.passes.size(), 1);
     if (!jit_enabled() || plan.passes.empty()) return;
     std::vector<Generated> gen = generate_plan(plan, true);
     if (compile_all(gen)) {
@@ -1130,6 +1185,7 @@ void jit_prepare(Plan& plan) {
 void jit_lookup(Plan& plan) {
     plan.jit.assign(plan.passes.size(), nullptr);
     plan.jit_aux.assign(plan.passes.size(), {});
+    plan.jit_tiles.assign(plan.passes.size(), 1);
     if (!jit_enabled() || plan.passes.empty()) return;
     {
         std::lock_guard<std::mutex> lock(g_cache_mu);
@@ -1146,14 +1202,16 @@ void jit_lookup(Plan& plan) {
 
 cudaError_t launch_plan_pass(const Plan& plan, size_t pass, void* amps, const FusedBatch* batch, cudaStream_t st) {
     const FusedPass& p = plan.passes[pass];
-    const void* kernel = pass < plan.jit.size() && pass < plan.jit_aux.size() && !plan.jit_aux[pass].empty()
+    const void* kernel = pass < plan.jit.size() && pass < plan.jit_aux.size() && pass < plan.jit_tiles.size() &&
+                                 !plan.jit_aux[pass].empty()
                              ? plan.jit[pass]
                              : nullptr;
     if (!kernel) return launch_fused(amps, plan.qubits, plan.precision, p, plan.d_ops, batch, st);
     if (batch && (batch->states < 1 || batch->states > 65535)) return cudaErrorInvalidValue;
     FusedLaunch L = fused_launch_params(plan.qubits, p, plan.d_ops, batch);
     const bool fp64 = plan.precision != QM_FP32;
-    const size_t smem = ((size_t)(fp64 ? 16 : 8) << p.k) + (((size_t)p.op_count * sizeof(FusedOp) + 15) & ~size_t(15)) +
+    const size_t smem = ((size_t)(fp64 ? 16 : 8) * (size_t)plan.jit_tiles[pass] << p.k) +
+                        (((size_t)p.op_count * sizeof(FusedOp) + 15) & ~size_t(15)) +
                         sizeof(double) * 8 * (size_t)L.table_slots;
     static const int sms = [] {
         int dev = 0, v = 0;

@@ -109,3 +109,25 @@ def test_compiled_passes_at_scale(gpu_context):
         got = st.Download()
     p.Dispose()
     assert np.max(np.abs(got - want)) <= 1e-12
+
+
+@pytest.mark.gpu
+def test_pipelined_complex64_passes(gpu_context):
+    """From 26 qubits complex64 passes copy the next tile into shared memory while the current
+    one computes; the state must match the complex128 passes (which load directly) to FP32
+    rounding."""
+    n = 26
+    c = brick_circuit(n, 6, seed=4)
+    _, _, _, launches0 = jit_info()
+    out = {}
+    for prec in (FP64, FP32):
+        p = Plan(gpu_context, c, prec, 0)
+        with DeviceState(gpu_context, n, prec) as st:
+            p.execute(st)
+            out[prec] = st.Download()
+        p.Dispose()
+    _, _, _, launches1 = jit_info()
+    assert launches1 > launches0
+    rel = np.linalg.norm(out[FP32] - out[FP64]) / np.linalg.norm(out[FP64])
+    assert rel <= 1e-5
+    assert abs(np.linalg.norm(out[FP32]) - 1.0) <= 1e-5
