@@ -879,8 +879,16 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int
     // 10.7 ms).  States of fewer than 26 qubits largely stay in L2, where the extra trip through
     // shared memory costs more than it hides, and passes with a batch table lose more from
     // reading it without staging: all of those load straight from global memory.
-    const bool piped = !fp64 && !tabled && qubits >= 26 && 2 * tile_bytes + prog_bytes <= (100u << 10);
-    const int tiles = piped ? 2 : 1;
+    const bool large = !tabled && qubits >= 26;
+    const bool second = large && !fp64 && 2 * tile_bytes + prog_bytes <= (100u << 10);
+    // Complex128: the exchange tile itself takes the next item's copy once the pass's last
+    // exchange is done, so the copy overlaps the ops after it, the flush and the stores.
+    const bool late = large && fp64;
+    const bool piped = second || late;
+    int last_stage = -1;
+    for (int o = 0; o < p.op_count; ++o)
+        if (plan_ops[(size_t)(p.op_begin + o)].code == OP_STAGE) last_stage = o;
+    const int tiles = second ? 2 : 1;
     // Blocks per SM: 128 registers per thread (512 threads per SM; fewer registers would spill
     // the 16 amplitudes) and the shared memory (a pipelined complex128 block of 12 qubits takes
     // an SM alone).
@@ -889,7 +897,8 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int
     std::ostringstream& os = g.os;  // the kernel body
     os << "extern __shared__ __align__(16) unsigned char smem_raw[];\n";
     os << "V* tile = reinterpret_cast<V*>(smem_raw);\n";
-    if (piped) os << "V* ptile = reinterpret_cast<V*>(smem_raw + " << tile_bytes << ");\n";
+    if (second) os << "V* ptile = reinterpret_cast<V*>(smem_raw + " << tile_bytes << ");\n";
+    if (late) os << "V* ptile = tile;\n";
     os << "FusedOp* prog = reinterpret_cast<FusedOp*>(smem_raw + " << tiles * tile_bytes << ");\n";
     os << "double* table = reinterpret_cast<double*>(smem_raw + " << (tiles * tile_bytes + prog_bytes) << ");\n";
     os << "const u32 t = threadIdx.x;\n";
@@ -943,8 +952,11 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int
         os << "{ const u32 sn = qm_swz(base);\n";
         for (int i = 0; i < NR; ++i)
             os << "{ const V v = ptile[sn ^ " << hexu(g.const_slot(i)) << "]; x" << i << " = v.x; y" << i << " = v.y; }\n";
-        os << "}\n__syncthreads();\n";
-        prefetch("item + gridDim.x");
+        os << "}\n";
+        if (second || last_stage < 0) {
+            os << "__syncthreads();\n";
+            prefetch("item + gridDim.x");
+        }
     } else {
         os << "{ const u32 g0 = outer | " << deposit_expr("t", thread_in) << ";\n";
         for (int i = 0; i < NR; ++i) {
@@ -960,6 +972,10 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int
         const FusedOp& op = plan_ops[(size_t)(p.op_begin + o)];
         if (op.code == OP_STAGE) {
             g.stage(op.reg_pos);
+            if (late && o == last_stage) {
+                os << "__syncthreads();\n";  // every thread has read the exchange tile
+                prefetch("item + gridDim.x");
+            }
             continue;
         }
         if (op.code == OP_DIAG_GROUP) {

@@ -112,12 +112,14 @@ def test_compiled_passes_at_scale(gpu_context):
 
 
 @pytest.mark.gpu
-def test_pipelined_complex64_passes(gpu_context):
-    """From 26 qubits complex64 passes copy the next tile into shared memory while the current
-    one computes; the state must match the complex128 passes (which load directly) to FP32
-    rounding."""
+def test_pipelined_passes(gpu_context):
+    """From 26 qubits compiled passes copy the next tile into shared memory while computing:
+    complex64 passes into a second tile, complex128 passes into the exchange tile after their
+    last exchange.  The complex128 state must match the oracle's parallel path, the complex64
+    one the complex128 one to FP32 rounding."""
     n = 26
-    c = brick_circuit(n, 6, seed=4)
+    c = brick_circuit(n, 4, seed=4)
+    want = orc.execute_parallel(c)
     _, _, _, launches0 = jit_info()
     out = {}
     for prec in (FP64, FP32):
@@ -128,6 +130,6 @@ def test_pipelined_complex64_passes(gpu_context):
         p.Dispose()
     _, _, _, launches1 = jit_info()
     assert launches1 > launches0
+    assert np.max(np.abs(out[FP64] - want)) <= 1e-12
     rel = np.linalg.norm(out[FP32] - out[FP64]) / np.linalg.norm(out[FP64])
     assert rel <= 1e-5
-    assert abs(np.linalg.norm(out[FP32]) - 1.0) <= 1e-5
