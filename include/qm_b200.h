@@ -239,7 +239,8 @@ int32_t qm_plan_program(int32_t qubits, int32_t precision, const qm_gate* gates,
 
 /* Passes compiled for their own op sequence.  Persistent plans (qm_plan_create), the batched
  * variational evaluator and the trajectory runner compile each distinct pass structure once
- * (NVRTC for sm_100a; coefficients stay data, so one kernel serves every angle) and run the
+ * (NVRTC for sm_100a; angles and the constants derived from them travel as kernel parameters,
+ * so a kernel serves every pass with its structure and rotation forms) and run the
  * compiled kernel; without NVRTC, or with QM_JIT=0 in the environment, they run the
  * interpreting pass kernel.  qm_jit_info reports whether compilation is available and the
  * process-wide counts; qm_jit_source returns the generated source of one pass of the plan the
