@@ -91,6 +91,64 @@ __global__ void __launch_bounds__(1 << (K - R), 512 / (1 << (K - R)))
             sign[u] = u < cnt ? P.t[k + u].sign : 0u;
             phase[u] = u < cnt ? P.t[k + u].phase : 0;
         }
+        // A Hermitian term (phase parity = parity of its Y count, as Pauli strings have) takes the
+        // same real part from index j and its partner j ^ F, so only the indices whose highest
+        // flip bit is 0 are summed, and doubled.  Each term's Z signs come from its sign mask over
+        // the tile's local bits plus one parity of the bits outside the tile; its phase is two
+        // flags.  Products and sums are FP64 for both precisions (exact products of complex64).
+        uint32_t sgl[kGroup], sbase[kGroup];
+        bool use_im[kGroup];
+        bool paired = flip != 0;
+#pragma unroll
+        for (int u = 0; u < kGroup; ++u) {
+            sgl[u] = 0u;
+            sbase[u] = 0u;
+            use_im[u] = false;
+            if (u < cnt) {
+                const uint32_t sg = P.t[k + u].sign;
+                uint32_t loc = 0, tm = P.thread_mask;
+                for (int b = 0; tm; ++b) {
+                    const uint32_t lowb = tm & (0u - tm);
+                    if (sg & lowb) loc |= 1u << b;
+                    tm ^= lowb;
+                }
+#pragma unroll
+                for (int m = 0; m < R; ++m)
+                    if (sg & P.reg_g[m]) loc |= 1u << (K - R + m);
+                const int ph = P.t[k + u].phase;
+                sgl[u] = loc;
+                use_im[u] = (ph & 1) != 0;
+                sbase[u] = ((ph == 1 || ph == 2) ? 1u : 0u) ^ ((uint32_t)__popc(sg & outer) & 1u);
+                if (((__popc(flip & loc) ^ ph) & 1) != 0) paired = false;
+            }
+        }
+        if (paired) {
+            const uint32_t pivot = 1u << (31 - __clz(flip));
+            const uint32_t below = pivot - 1u;
+            double hacc[kGroup] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+            for (int r = 0; r < NR / 2; ++r) {
+                const uint32_t h = t + (uint32_t)NT * r;
+                const uint32_t j = (h & below) | ((h & ~below) << 1);
+                const V a = tile[j], b = tile[j ^ flip];
+                const double ar = a.x, ai = a.y, br = b.x, bi = b.y;
+                const double ore = br * ar + bi * ai, oim = br * ai - bi * ar;
+#pragma unroll
+                for (int u = 0; u < kGroup; ++u) {
+                    if (u >= cnt) break;
+                    const double c = use_im[u] ? oim : ore;
+                    hacc[u] += ((__popc(j & sgl[u]) ^ sbase[u]) & 1u) ? -c : c;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kGroup; ++u) {
+                if (u >= cnt) break;
+                const double v = warp_sum(2.0 * hacc[u]);
+                if (lane == 0) red[warp * (P.terms + 1) + k + u] = v;
+            }
+            k += cnt;
+            continue;
+        }
         double acc[kGroup] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
         for (int i = 0; i < NR; ++i) {
