@@ -282,6 +282,12 @@ int32_t qm_expectation_pauli(qm_state* state, const qm_pauli_term* terms, int32_
  * with Neumaier compensation.  An empty term list still validates the mass. */
 int32_t qm_expectation_energy(qm_state* state, const qm_pauli_term* terms, int32_t count,
                               double* energy);
+/* The batched variational evaluator compiles the tiled expectation for its term list (one
+ * kernel per tile pass: flip masks, phases and tile-local signs as constants).  Returns the
+ * generated source of tile pass `pass` for these terms on a `qubits`-qubit state (inspection
+ * and tests; length receives the full size).  No reference counterpart. */
+int32_t qm_jit_expect_source(int32_t qubits, int32_t precision, const qm_pauli_term* terms, int32_t count,
+                             int32_t pass, char* buffer, size_t size, size_t* length);
 
 /* ---------------------------------------------------------------- sampling */
 

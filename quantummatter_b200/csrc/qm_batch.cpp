@@ -127,9 +127,13 @@ cudaError_t enqueue_tile_expectation(const void* amps, int qubits, int precision
                                      double* partials, double* out, cudaStream_t st) {
     const size_t partial = sizeof(double) * (size_t)states * tp.rows_per_state * tp.columns;
     cudaError_t e = cudaMemsetAsync(partials, 0, partial, st);
-    for (size_t i = 0; e == cudaSuccess && i < tp.passes.size(); ++i)
-        e = launch_expect_tile(amps, qubits, precision, tp.passes[i], tp.terms.data(), states, (uint64_t)1 << qubits,
-                               partials, tp.columns, tp.rows_per_state, tp.mass_column, st);
+    for (size_t i = 0; e == cudaSuccess && i < tp.passes.size(); ++i) {
+        const void* k = i < tp.jit.size() ? tp.jit[i] : nullptr;
+        e = k ? launch_expect_tile_jit(k, amps, qubits, precision, tp.passes[i], states, (uint64_t)1 << qubits, partials,
+                                       tp.columns, tp.rows_per_state, tp.mass_column, st)
+              : launch_expect_tile(amps, qubits, precision, tp.passes[i], tp.terms.data(), states, (uint64_t)1 << qubits,
+                                   partials, tp.columns, tp.rows_per_state, tp.mass_column, st);
+    }
     if (e == cudaSuccess) e = launch_finish_batched(partials, states, tp.rows_per_state, tp.columns, out, st);
     return e;
 }
@@ -478,6 +482,7 @@ int32_t vqe_evaluate(qm_context* ctx, int32_t qubits, int32_t precision, const q
     }
     TilePlan tp;
     if (!plan_tiles(qubits, precision, terms, term_count, tp, err)) return fail(QM_E_ARG, err);
+    jit_prepare_tiles(tp, qubits, precision);  // one term list for every circuit of every wave
 
     const int64_t state_bytes = (precision == QM_FP32 ? 8ll : 16ll) << qubits;
     const int64_t free_budget = ctx->device_budget - ctx->device_in_use;

@@ -232,7 +232,13 @@ struct TilePlan {
     int32_t rows_per_state = 0;
     int32_t columns = 0;         // terms + 1 (the mass)
     int32_t mass_column = 0;
+    std::vector<const void*> jit;  // per pass: the kernel compiled for its term list, or null
 };
+// Compiles each tile pass's term list (NVRTC; cached by source) / launches one compiled pass.
+void jit_prepare_tiles(TilePlan& plan, int qubits, int precision);
+cudaError_t launch_expect_tile_jit(const void* kernel, const void* amps, int qubits, int precision, const TilePass& pass,
+                                   int states, uint64_t state_stride, double* partials, int columns, int rows_per_state,
+                                   int mass_column, cudaStream_t s);
 int tile_block_qubits(int qubits, int precision);
 bool plan_tiles(int qubits, int precision, const qm_pauli_term* terms, int count, TilePlan& plan, std::string& error);
 cudaError_t launch_expect_tile(const void* amps, int qubits, int precision, const TilePass& pass, const TileTerm* terms,

@@ -1084,7 +1084,8 @@ cudaKernel_t compile_source(const std::string& src) {
             if (n.cubin(prog, cubin.data()) == NVRTC_SUCCESS) {
                 cudaLibrary_t lib = nullptr;
                 if (cudaLibraryLoadData(&lib, cubin.data(), nullptr, nullptr, 0, nullptr, nullptr, 0) == cudaSuccess &&
-                    cudaLibraryGetKernel(&kernel, lib, "qm_pass") == cudaSuccess) {
+                    cudaLibraryGetKernel(&kernel, lib, src.find("qm_expect(") != std::string::npos ? "qm_expect" : "qm_pass") ==
+                        cudaSuccess) {
                     int dev = 0, optin = 0;
                     if (cudaGetDevice(&dev) != cudaSuccess ||
                         cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
@@ -1250,7 +1251,259 @@ cudaError_t launch_plan_pass(const Plan& plan, size_t pass, void* amps, const Fu
     return e;
 }
 
+// ---------------------------------------------------------------- tiled expectation, compiled
+// The tiled expectation kernel (qm_expect.cu) generated for one tile pass's term list: flip
+// masks, pivots, phases and the tile-local Z-sign bits are constants, so a flip group's loop is
+// two shared loads, the FP64 overlap and one add or subtract per term.  The reduction order and
+// the partial-table layout are those of the generic kernel.
+namespace {
+
+uint32_t insert_zero(uint32_t v, int bit) {
+    const uint32_t below = (1u << bit) - 1u;
+    return (v & below) | ((v & ~below) << 1);
+}
+
+std::string generate_expect(int qubits, bool fp64, const TilePass& tp, const TileTerm* all_terms) {
+    const int K = tp.k, NT = 1 << (K - R), WARPS = NT / 32;
+    const int T = tp.term_count;
+    const TileTerm* terms = all_terms + tp.term_begin;
+    const int NCOL = T + 1;
+    uint32_t thread_mask = 0, reg_g[R];
+    for (int b = 0; b < K - R; ++b) thread_mask |= 1u << tp.q[b];
+    for (int m = 0; m < R; ++m) reg_g[m] = 1u << tp.q[K - R + m];
+    const uint32_t all = qubits >= 32 ? 0xffffffffu : ((1u << qubits) - 1u);
+    const uint32_t outer_all = all & ~tp.block_mask;
+    auto local_of = [&](uint32_t global) {
+        uint32_t l = 0;
+        for (int b = 0; b < K; ++b)
+            if (global & (1u << tp.q[b])) l |= 1u << b;
+        return l;
+    };
+    const uint32_t lo_mask = (1u << (K - R)) - 1u;
+    int ndiag = 0;
+    while (ndiag < T && terms[ndiag].flip_local == 0) ++ndiag;
+    const bool wht = ndiag >= 3;
+
+    std::ostringstream os;
+    os << "typedef unsigned int u32;\ntypedef unsigned long long u64;\n";
+    os << "typedef " << (fp64 ? "double2" : "float2") << " V;\n";
+    os << "struct ExpLaunch { u32 outer_mask; int row_offset; int rows_per_state; int columns; int mass_column; int pad;\n"
+          "  u64 state_stride; double* partials; };\n";
+    os << "__device__ __forceinline__ u32 qm_deposit(u32 value, u32 mask) {\n"
+          "  u32 out = 0;\n"
+          "  while (mask) { const u32 low = mask & (0u - mask); if (value & 1u) out |= low; value >>= 1; mask ^= low; }\n"
+          "  return out;\n}\n";
+    os << "__device__ __forceinline__ double warp_sum(double v) {\n"
+          "  for (int d = 16; d > 0; d >>= 1) v += __shfl_down_sync(0xffffffffu, v, d);\n  return v;\n}\n";
+    // per-term constants of the final write
+    os << "__constant__ int c_col[" << std::max(1, T) << "] = {";
+    for (int k = 0; k < T; ++k) os << (k ? ", " : "") << terms[k].column;
+    os << "};\n__constant__ u32 c_loc[" << std::max(1, T) << "] = {";
+    for (int k = 0; k < T; ++k) os << (k ? ", " : "") << hexu(local_of(terms[k].sign & tp.block_mask));
+    os << "};\n__constant__ u32 c_sout[" << std::max(1, T) << "] = {";
+    for (int k = 0; k < T; ++k) os << (k ? ", " : "") << hexu(terms[k].sign & outer_all);
+    os << "};\n";
+    os << "extern \"C\" __global__ void __launch_bounds__(" << NT << ", " << std::max(1, 512 / NT)
+       << ") qm_expect(const V* __restrict__ s, const __grid_constant__ ExpLaunch P) {\n";
+    os << "extern __shared__ __align__(16) unsigned char smem_raw[];\n";
+    os << "V* tile = reinterpret_cast<V*>(smem_raw);\n";
+    os << "double* red = reinterpret_cast<double*>(smem_raw + " << ((fp64 ? 16 : 8) << K) << ");\n";
+    os << "const u32 t = threadIdx.x;\nconst int warp = t >> 5, lane = t & 31;\n(void)warp; (void)lane;\n";
+    os << "s += (u64)blockIdx.y * P.state_stride;\n";
+    os << "const u32 outer = qm_deposit(blockIdx.x, P.outer_mask);\n";
+    os << "{ const u32 g0 = outer | " << deposit_expr("t", thread_mask) << ";\n";
+    for (int i = 0; i < NR; ++i) {
+        uint32_t off = 0;
+        for (int m = 0; m < R; ++m)
+            if ((i >> m) & 1) off |= reg_g[m];
+        os << "tile[t | " << hexu((uint32_t)i << (K - R)) << "] = s[g0 | " << hexu(off) << "];\n";
+    }
+    os << "}\n__syncthreads();\n";
+
+    // flip groups (and diagonal terms when fewer than three), at most 8 terms per loop
+    for (int k = wht ? ndiag : 0; k < T;) {
+        const uint32_t F = terms[k].flip_local;
+        int cnt = 1;
+        while (cnt < 8 && k + cnt < T && terms[k + cnt].flip_local == F) ++cnt;
+        bool paired = F != 0;
+        for (int u = 0; u < cnt; ++u) {
+            const uint32_t sl = local_of(terms[k + u].sign & tp.block_mask);
+            if (((__builtin_popcount(F & sl) ^ terms[k + u].phase) & 1) != 0) paired = false;
+        }
+        os << "{\n";
+        for (int u = 0; u < cnt; ++u) os << "double a" << u << " = 0.0;\n";
+        auto term_add = [&](int u, uint32_t j_const, const char* ore, const char* oim) {
+            const TileTerm& tt = terms[k + u];
+            const uint32_t sl = local_of(tt.sign & tp.block_mask);
+            const bool neg = (tt.phase == 1 || tt.phase == 2) ^ (__builtin_popcount(j_const & sl) & 1);
+            os << "a" << u << (neg ? " -= " : " += ") << ((tt.phase & 1) ? oim : ore) << ";\n";
+        };
+        std::string jt;
+        uint32_t jt_bits = lo_mask;  // local bits the run-time index part can hold
+        if (paired) {
+            const int pivot = 31 - __builtin_clz(F);
+            if (pivot >= K - R) {
+                jt = "t";
+            } else {
+                jt_bits = (lo_mask << 1) | 1u;  // the thread index with a zero inserted at the pivot
+                const uint32_t below = (1u << pivot) - 1u;
+                os << "const u32 jt = (t & " << hexu(below) << ") | ((t & " << hexu(~below & lo_mask) << ") << 1);\n";
+                jt = "jt";
+            }
+            for (int r = 0; r < NR / 2; ++r) {
+                const uint32_t c = insert_zero((uint32_t)(NT * r), pivot);
+                os << "{ const V a = tile[" << jt << " | " << hexu(c) << "], b = tile[(" << jt << " | " << hexu(c) << ") ^ "
+                   << hexu(F) << "];\n";
+                os << "const double ar = a.x, ai = a.y, br = b.x, bi = b.y;\n";
+                os << "const double ore = br * ar + bi * ai, oim = br * ai - bi * ar;\n";
+                for (int u = 0; u < cnt; ++u) term_add(u, c, "ore", "oim");
+                os << "}\n";
+            }
+        } else {
+            jt = "t";
+            for (int i = 0; i < NR; ++i) {
+                const uint32_t c = (uint32_t)i << (K - R);
+                os << "{ const V a = tile[t | " << hexu(c) << "];\nconst double ar = a.x, ai = a.y;\n";
+                if (F == 0) {
+                    os << "const double ore = ar * ar + ai * ai, oim = 0.0;\n";
+                } else {
+                    os << "const V b = tile[(t | " << hexu(c) << ") ^ " << hexu(F) << "];\nconst double br = b.x, bi = b.y;\n";
+                    os << "const double ore = br * ar + bi * ai, oim = br * ai - bi * ar;\n";
+                }
+                for (int u = 0; u < cnt; ++u) term_add(u, c, "ore", "oim");
+                os << "}\n";
+            }
+        }
+        for (int u = 0; u < cnt; ++u) {
+            const TileTerm& tt = terms[k + u];
+            const uint32_t sl = local_of(tt.sign & tp.block_mask) & jt_bits;  // run-time part of the local sign
+            const uint32_t so = tt.sign & outer_all;
+            std::string par;
+            if (sl) par = "__popc(" + jt + " & " + hexu(sl) + ")";
+            if (so) par += std::string(par.empty() ? "" : " + ") + "__popc(outer & " + hexu(so) + ")";
+            const char* scale = paired ? "2.0" : "1.0";
+            if (par.empty())
+                os << "{ const double v = warp_sum(" << scale << " * a" << u << ");\n";
+            else
+                os << "{ const double v = warp_sum(((" << par << ") & 1) ? -" << scale << " * a" << u << " : " << scale
+                   << " * a" << u << ");\n";
+            os << "if (lane == 0) red[warp * " << NCOL << " + " << (k + u) << "] = v; }\n";
+        }
+        os << "}\n";
+        k += cnt;
+    }
+    if (tp.with_mass) {
+        os << "{ double m = 0.0;\n";
+        for (int i = 0; i < NR; ++i)
+            os << "{ const V a = tile[t | " << hexu((uint32_t)i << (K - R)) << "]; m += (double)a.x * a.x + (double)a.y * a.y; }\n";
+        os << "m = warp_sum(m);\nif (lane == 0) red[warp * " << NCOL << " + " << T << "] = m; }\n";
+    }
+    if (wht) {
+        // Walsh-Hadamard transform of the tile's Born probabilities (as the generic kernel)
+        os << "double* wbuf = reinterpret_cast<double*>(smem_raw);\n{\ndouble w[" << NR << "];\n";
+        for (int i = 0; i < NR; ++i)
+            os << "{ const V a = tile[t | " << hexu((uint32_t)i << (K - R)) << "]; w[" << i
+               << "] = (double)a.x * a.x + (double)a.y * a.y; }\n";
+        for (int m = 0; m < R; ++m)
+            for (int i = 0; i < NR; ++i)
+                if (!((i >> m) & 1))
+                    os << "{ const double x = w[" << i << "], y = w[" << (i | (1 << m)) << "]; w[" << i << "] = x + y; w["
+                       << (i | (1 << m)) << "] = x - y; }\n";
+        for (int m = 0; m < 5; ++m) {
+            os << "#pragma unroll\nfor (int i = 0; i < " << NR << "; ++i) { const double y = __shfl_xor_sync(0xffffffffu, w[i], "
+               << (1 << m) << "); w[i] = ((lane >> " << m << ") & 1) ? y - w[i] : w[i] + y; }\n";
+        }
+        os << "__syncthreads();\n";
+        os << "#pragma unroll\nfor (int i = 0; i < " << NR << "; ++i) wbuf[t | ((u32)i << " << (K - R) << ")] = w[i];\n";
+        for (int m = 5; m < K - R; ++m) {
+            os << "__syncthreads();\n#pragma unroll\nfor (int i = 0; i < " << NR << "; ++i) { const u32 j = t | ((u32)i << "
+               << (K - R) << "); const double x = wbuf[j], y = wbuf[j ^ " << (1u << m) << "u]; w[i] = ((j >> " << m
+               << ") & 1u) ? y - x : x + y; }\n";
+            os << "__syncthreads();\n#pragma unroll\nfor (int i = 0; i < " << NR << "; ++i) wbuf[t | ((u32)i << " << (K - R)
+               << ")] = w[i];\n";
+        }
+        os << "}\n";
+    }
+    os << "__syncthreads();\n";
+    os << "const u64 row = (u64)blockIdx.y * P.rows_per_state + P.row_offset + blockIdx.x;\n";
+    os << "for (int k = t; k < " << (T + (tp.with_mass ? 1 : 0)) << "; k += " << NT << ") {\n";
+    os << "double sum = 0.0;\n";
+    if (wht) {
+        os << "if (k < " << ndiag << ") { sum = reinterpret_cast<const double*>(smem_raw)[c_loc[k]];\n"
+              "  if (__popc(outer & c_sout[k]) & 1) sum = -sum;\n"
+              "  P.partials[row * P.columns + c_col[k]] = sum; continue; }\n";
+    }
+    os << "for (int w = 0; w < " << WARPS << "; ++w) sum += red[w * " << NCOL << " + k];\n";
+    os << "const int col = k < " << T << " ? c_col[k < " << T << " ? k : 0] : P.mass_column;\n";
+    os << "P.partials[row * P.columns + col] = sum;\n}\n}\n";
+    return os.str();
+}
+
+struct ExpLaunchHost {
+    uint32_t outer_mask;
+    int32_t row_offset, rows_per_state, columns, mass_column, pad;
+    uint64_t state_stride;
+    double* partials;
+};
+static_assert(sizeof(ExpLaunchHost) == 40, "ExpLaunch layout is mirrored in the generated source");
+
+}  // namespace
+
+void jit_prepare_tiles(TilePlan& tp, int qubits, int precision) {
+    tp.jit.assign(tp.passes.size(), nullptr);
+    if (!jit_enabled() || tp.passes.empty()) return;
+    std::vector<Generated> gen(tp.passes.size());
+    for (size_t i = 0; i < tp.passes.size(); ++i)
+        gen[i].src = generate_expect(qubits, precision != QM_FP32, tp.passes[i], tp.terms.data());
+    compile_all(gen);
+    for (size_t i = 0; i < gen.size(); ++i) tp.jit[i] = reinterpret_cast<const void*>(kernel_for(gen[i].src));
+}
+
+cudaError_t launch_expect_tile_jit(const void* kernel, const void* amps, int qubits, int precision, const TilePass& tp,
+                                   int states, uint64_t state_stride, double* partials, int columns, int rows_per_state,
+                                   int mass_column, cudaStream_t st) {
+    if (states < 1 || states > 65535) return cudaErrorInvalidValue;
+    ExpLaunchHost L{};
+    const uint32_t all = qubits >= 32 ? 0xffffffffu : ((1u << qubits) - 1u);
+    L.outer_mask = all & ~tp.block_mask;
+    L.row_offset = tp.row_offset;
+    L.rows_per_state = rows_per_state;
+    L.columns = columns;
+    L.mass_column = mass_column;
+    L.state_stride = state_stride;
+    L.partials = partials;
+    const int K = tp.k;
+    const size_t smem = ((size_t)(precision == QM_FP32 ? 8 : 16) << K) +
+                        sizeof(double) * (size_t)((1 << (K - R)) / 32) * (size_t)(tp.term_count + 1);
+    const void* arg0 = amps;
+    void* args[] = {&arg0, &L};
+    dim3 grid(1u << (qubits - K), (unsigned)states);
+    const cudaError_t e = cudaLaunchKernel(kernel, grid, dim3(1u << (K - R)), args, smem, st);
+    if (e == cudaSuccess) ++g_launches;
+    return e;
+}
+
 }  // namespace qm
+
+extern "C" int32_t qm_jit_expect_source(int32_t qubits, int32_t precision, const qm_pauli_term* terms, int32_t count,
+                                        int32_t pass, char* buffer, size_t size, size_t* length) {
+    using namespace qm;
+    if (qubits < 9 || qubits > 30) return fail(QM_E_RANGE, "tiled expectations need 9 to 30 qubits");
+    if (precision != QM_FP64 && precision != QM_FP32) return fail(QM_E_RANGE, "unknown precision");
+    if (count < 0 || (count > 0 && !terms)) return fail(QM_E_ARG, "bad term list");
+    TilePlan tp;
+    std::string err;
+    if (!plan_tiles(qubits, precision, terms, count, tp, err)) return fail(QM_E_ARG, err);
+    if (pass < 0 || (size_t)pass >= tp.passes.size()) return fail(QM_E_RANGE, "pass index out of range");
+    const std::string src = generate_expect(qubits, precision != QM_FP32, tp.passes[(size_t)pass], tp.terms.data());
+    if (length) *length = src.size();
+    if (buffer && size) {
+        const size_t n = std::min(size - 1, src.size());
+        std::memcpy(buffer, src.data(), n);
+        buffer[n] = '\0';
+    }
+    return QM_OK;
+}
 
 extern "C" int32_t qm_jit_info(int32_t* available, int64_t* kernels, int64_t* failed, int64_t* launches) {
     if (available) *available = qm::jit_enabled() ? 1 : 0;

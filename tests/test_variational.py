@@ -172,3 +172,49 @@ def test_fp32_energies_within_1e6_of_the_fp64_oracle(gpu_context):
     for v in range(4):
         want = ref.energy(c, h, params[v])
         assert abs(fp32.Energies[v] - want) <= 1e-6, (fp32.Energies[v], want)
+
+
+def structured_hamiltonian(qubits: int, diagonal: int, seed: int) -> PauliHamiltonian:
+    """Terms that reach every branch of the tiled expectation compiled for a term list: flips
+    whose highest bit is a thread bit of the tile (a zero is inserted below the register bits)
+    with Z/Y on the bits just above; more than eight terms sharing one flip mask; flips on
+    register bits; and `diagonal` Z-only terms (fewer than three, or a Walsh-Hadamard set)."""
+    rng = np.random.default_rng(seed)
+    terms = []
+
+    def add(ops):
+        lab = ["I"] * qubits
+        for q, p in ops.items():
+            lab[qubits - 1 - q] = p
+        terms.append(PauliTerm(float(rng.normal()), PauliString("".join(lab))))
+
+    for z in range(10):  # one flip mask {0, 1}, ten Z patterns above it
+        ops = {0: "X", 1: "Y" if z % 2 else "X"}
+        for q in range(2, qubits):
+            if (z >> (q % 4)) & 1:
+                ops[q] = "Z"
+        add(ops)
+    for q in range(qubits - 1):  # X/Y pairs on every bond, Z on the qubit after
+        add({q: "X", q + 1: "X"})
+        add({q: "Y", q + 1: "Y", (q + 2) % qubits: "Z"} if q + 2 < qubits else {q: "Y", q + 1: "Y"})
+    for d in range(diagonal):
+        add({d % qubits: "Z", (3 * d + 1) % qubits: "Z"} if d % 2 else {(5 * d) % qubits: "Z"})
+    return PauliHamiltonian(qubits, terms)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("diagonal", [2, 6])
+@pytest.mark.parametrize("fp32", [False, True])
+def test_compiled_tile_expectation_matches_the_oracle(gpu_context, diagonal, fp32):
+    from quantummatter_b200.backend import FP32, FP64
+    from quantummatter_b200.variational import B200VariationalEnergyEvaluator
+    n = 14
+    c = hardware_efficient_ansatz(n, 2)
+    h = structured_hamiltonian(n, diagonal, seed=diagonal)
+    params = uniform_parameters(c.ParameterCount, 3, -math.pi, math.pi, seed=14)
+    ev = B200VariationalEnergyEvaluator(gpu_context, FP32 if fp32 else FP64)
+    got = ev.EvaluateBatch(c, h, params, withGradient=False)
+    scale = max(1.0, sum(abs(t.Coefficient) for t in h.Terms))
+    for v in range(3):
+        want = ref.energy(c, h, params[v])
+        assert abs(got.Energies[v] - want) <= (1e-6 if fp32 else 5e-12) * scale, (v, got.Energies[v], want)
