@@ -212,8 +212,13 @@ def test_compiled_tile_expectation_matches_the_oracle(gpu_context, diagonal, fp3
     c = hardware_efficient_ansatz(n, 2)
     h = structured_hamiltonian(n, diagonal, seed=diagonal)
     params = uniform_parameters(c.ParameterCount, 3, -math.pi, math.pi, seed=14)
+    from quantummatter_b200.backend import jit_info
     ev = B200VariationalEnergyEvaluator(gpu_context, FP32 if fp32 else FP64)
+    before = jit_info()
     got = ev.EvaluateBatch(c, h, params, withGradient=False)
+    after = jit_info()
+    # passes and tile expectations ran compiled, none failed
+    assert after["failed"] == before["failed"] and after["launches"] > before["launches"]
     scale = max(1.0, sum(abs(t.Coefficient) for t in h.Terms))
     for v in range(3):
         want = ref.energy(c, h, params[v])
