@@ -260,6 +260,12 @@ int32_t qm_apply_pauli(qm_state* state, int32_t target, int32_t pauli);
  * psi0 = jump_scale * psi1, psi1 = 0; otherwise psi0 *= scale, psi1 *= stay_scale. */
 int32_t qm_apply_damping(qm_state* state, int32_t target, int32_t jump, double scale,
                          double jump_scale, double stay_scale);
+/* INoiseChannelBackend.Apply on a resident state: qm_noise_apply_host's branch choice and draw
+ * consumption (none when p == 0, none for a flip with p == 1, none for damping when either
+ * branch has zero mass), with no copy of the state.  The device-resident noisy dynamic circuit
+ * uses it between segments. */
+int32_t qm_state_noise_apply(qm_state* state, int32_t kind, double probability, int32_t target,
+                             qm_next_double_fn next_double, void* user);
 
 /* ---------------------------------------------------------------- observables */
 

@@ -390,6 +390,26 @@ class DeviceState:
     def ApplyDamping(self, target: int, jump: bool, scale: float, jump_scale: float, stay_scale: float) -> None:
         check(load().qm_apply_damping(self.handle, target, 1 if jump else 0, scale, jump_scale, stay_scale))
 
+    def ApplyNoise(self, channel, target: int, random) -> None:
+        """INoiseChannelBackend.Apply on the resident state (qm_state_noise_apply): `random` is
+        any object with NextDouble(), consumed exactly where the reference consumes it."""
+        if channel is None or random is None:
+            raise ArgumentError("channel and random are required")
+        errors: list[BaseException] = []
+
+        def draw(_user):
+            try:
+                return float(random.NextDouble())
+            except BaseException as exc:  # surfaced after the call returns
+                errors.append(exc)
+                return 0.0
+
+        cb = _lib.NEXT_DOUBLE_FN(draw)
+        rc = load().qm_state_noise_apply(self.handle, int(channel.Kind), float(channel.Probability), target, cb, None)
+        if errors:
+            raise errors[0]
+        check(rc)
+
     # -- sampling
     def MeasureAll(self, u: float) -> tuple[int, bool]:
         out, amb = C.c_int64(), C.c_int32()

@@ -920,6 +920,37 @@ extern "C" int32_t qm_apply_damping(qm_state* st, int32_t target, int32_t jump, 
     return QM_OK;
 }
 
+extern "C" int32_t qm_state_noise_apply(qm_state* st, int32_t kind, double p, int32_t target,
+                                        qm_next_double_fn next_double, void* user) {
+    int32_t rc = check_state(st);
+    if (rc) return rc;
+    if (!next_double) return fail(QM_E_ARG, "random source is null");
+    if (kind < 0 || kind > 3) return fail(QM_E_RANGE, "unknown noise kind");
+    if (!std::isfinite(p) || p < 0 || p > 1) return fail(QM_E_RANGE, "Channel probability must be finite and in [0,1].");
+    if ((uint32_t)target >= (uint32_t)st->qubits) return fail(QM_E_RANGE, "target out of range");
+    if (p == 0) return QM_OK;
+    auto draw = [&]() { return next_double(user); };
+    std::lock_guard<std::recursive_mutex> lock(st->ctx->mu);
+    QM_CUDA(cudaSetDevice(st->ctx->device));
+    Branch b;
+    if (kind != 3) {
+        rc = choose_branch(kind, p, draw, false, 0, 0, b);
+        if (rc) return rc;
+        if (b.pauli == 0) return QM_OK;
+        QM_CUDA(launch_pauli(st->amps, st->qubits, st->precision, target, b.pauli, st->ctx->stream));
+    } else {
+        double m0 = 0, m1 = 0;
+        rc = device_masses(st->ctx, st->amps, st->qubits, st->precision, target, &m0, &m1);
+        if (rc) return rc;
+        rc = choose_branch(kind, p, draw, true, m0, m1, b);
+        if (rc) return rc;
+        QM_CUDA(launch_damping(st->amps, st->qubits, st->precision, target, b.jump ? 1 : 0, b.scale, b.jump_scale,
+                               b.stay_scale, st->ctx->stream));
+    }
+    QM_CUDA(cudaStreamSynchronize(st->ctx->stream));
+    return QM_OK;
+}
+
 // ====================================================================== observables
 
 namespace {

@@ -6,7 +6,7 @@ import pytest
 
 import oracle as orc
 from circuits import random_state
-from dynamic_ref import execute, layered, teleportation
+from dynamic_ref import execute, layered, noisy_layered, noisy_teleportation, teleportation
 from quantummatter_b200.backend import FP32, FP64, DeviceState
 from quantummatter_b200.dynamic import B200DynamicSimulator
 from quantummatter_b200.errors import ArgumentError, ArgumentOutOfRangeError, MassError
@@ -71,5 +71,35 @@ def test_simulate_trajectory_state(gpu_context):
     dc = layered(10, 9)
     t = B200DynamicSimulator(gpu_context).SimulateTrajectory(dc, seed=3)
     state, classical = execute(dc, random_doubles(3, dc.DrawsPerExecution()))
+    assert t.ClassicalRegister == classical
+    assert np.max(np.abs(t.FinalState - state)) <= 1e-12
+
+
+@pytest.mark.parametrize("build,n", [(lambda: noisy_teleportation(), 3), (lambda: noisy_layered(12, 6), 12)])
+def test_noisy_dynamic_run_counts_follow_the_reference(gpu_context, build, n):
+    """Noise placements between dynamic instructions, applied on the resident state, take the
+    same branches and draws as the oracle composition over one seeded stream across shots."""
+    from dynamic_ref import execute_noisy
+    from quantummatter_b200.dynamic import B200NoisyDynamicSimulator
+    nd = build()
+    shots, seed = 40, 7
+    res = B200NoisyDynamicSimulator(gpu_context).Run(nd, shots=shots, seed=seed)
+    draws = random_doubles(seed, 40 * 64)
+    want, k = {}, 0
+    for _ in range(shots):
+        _, classical, used = execute_noisy(nd, draws[k:])
+        k += used
+        key = format(classical, "b").zfill(nd.ClassicalBitCount)
+        want[key] = want.get(key, 0) + 1
+    assert res.Ambiguous == 0
+    assert res.Counts == dict(sorted(want.items()))
+
+
+def test_noisy_dynamic_trajectory_state(gpu_context):
+    from dynamic_ref import execute_noisy
+    from quantummatter_b200.dynamic import B200NoisyDynamicSimulator
+    nd = noisy_layered(10, 11)
+    t = B200NoisyDynamicSimulator(gpu_context).SimulateTrajectory(nd, seed=5)
+    state, classical, _ = execute_noisy(nd, random_doubles(5, 256))
     assert t.ClassicalRegister == classical
     assert np.max(np.abs(t.FinalState - state)) <= 1e-12

@@ -90,3 +90,36 @@ def test_teleportation_moves_the_state():
         dc2._steps.append(step)
     state, _ = execute(dc2, [0.3, 0.7, 0.2])
     assert orc.marginal_probability(state, [2], 1) == pytest.approx(np.sin(0.55) ** 2, abs=1e-12)
+
+
+def test_noisy_dynamic_builder():
+    """NoisyDynamicCircuit validates each instruction before taking it; channels are checked as
+    NoisyCircuit.ApplyNoise checks them, and a rejected instruction changes nothing."""
+    from quantummatter_b200.dynamic import MeasurementStep, NoiseStep, NoisyDynamicCircuit, UnitaryStep
+    from quantummatter_b200.noise import NoiseChannel
+    nd = NoisyDynamicCircuit(3, 2)
+    nd.Append(QuantumCircuit(3).H(0)).ApplyNoise(NoiseChannel.Depolarizing(0.1), 2).Measure([0], [1])
+    assert nd.StepCount == 3
+    kinds = [type(s) for s in nd.Steps]
+    assert kinds == [UnitaryStep, NoiseStep, MeasurementStep]
+    with pytest.raises(ArgumentOutOfRangeError):
+        nd.ApplyNoise(NoiseChannel.BitFlip(0.1), 3)
+    with pytest.raises(ArgumentError):
+        nd.ApplyNoise(None, 0)
+    with pytest.raises(ArgumentError):
+        nd.Append(QuantumCircuit(2).H(0))
+    with pytest.raises(ArgumentOutOfRangeError):
+        nd.If(4, 0, QuantumCircuit(3))
+    assert nd.StepCount == 3
+    with pytest.raises(ArgumentOutOfRangeError):
+        NoisyDynamicCircuit(0, 1)
+
+
+def test_noisy_dynamic_reference_composition_consumes_draws_like_the_reference():
+    """The oracle composition takes no draw for p = 0 and for a flip with p = 1."""
+    from dynamic_ref import execute_noisy, noisy_teleportation
+    nd = noisy_teleportation()
+    draws = np.random.default_rng(4).random(64)
+    _, _, used = execute_noisy(nd, draws)
+    # depolarizing, damping (both branches carry mass here), two measurements, reset, flip 0.25
+    assert used == 6
