@@ -111,6 +111,12 @@ struct Plan {
     std::vector<const void*> jit;   // per pass: compiled kernel (cudaKernel_t) or null
     std::vector<std::vector<unsigned char>> jit_aux;  // per pass: the compiled kernel's constants
     std::vector<int> jit_tiles;     // per pass: shared-memory tiles of the compiled kernel (2: pipelined)
+    std::vector<int> jit_hist_bins; // per pass: bins of the compiled kernel's joint-mass epilogue (0: none)
+    // Joint masses over these qubits (at most 8) are wanted after the plan (a damping group of the
+    // trajectory runner): the last pass computes them in its epilogue when it compiles
+    // (hist_fused), in the layout of launch_group_histogram.
+    uint32_t hist_mask = 0;
+    bool hist_fused = false;
     bool borrowed = false;          // d_ops belongs to a context buffer
     int64_t planned_bytes = 0;
     int32_t launches = 0;
@@ -141,6 +147,7 @@ struct FusedBatch {
     uint64_t table_stride;
     int32_t slot_offset = 0;
     int32_t slot_count = -1;
+    double* hist = nullptr;  // joint-mass partial rows written by a compiled pass with a histogram epilogue
 };
 cudaError_t launch_fused(void* amps, int qubits, int precision, const FusedPass& p, const FusedOp* ops,
                          const FusedBatch* batch, cudaStream_t s);

@@ -835,10 +835,11 @@ struct Generated {
     std::string src;
     std::vector<unsigned char> aux;  // the parameter block: doubles (complex128) or floats
     int tiles = 1;                   // tiles of shared memory (2: pipelined)
+    int hist_bins = 0;               // joint-mass epilogue bins (0: none)
 };
 
 Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int qubits, bool fp64, Carry* carry,
-                   bool last) {
+                   bool last, uint32_t hist_mask = 0) {
     Gen g;
     g.fp64 = fp64;
     g.K = p.k;
@@ -879,7 +880,16 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int
     // 10.7 ms).  States of fewer than 26 qubits largely stay in L2, where the extra trip through
     // shared memory costs more than it hides, and passes with a batch table lose more from
     // reading it without staging: all of those load straight from global memory.
-    const bool large = !tabled && qubits >= 26;
+    // Joint-mass epilogue: work items go in chunks of C consecutive tiles of one state, so that
+    // partial row u = state * rows + r always holds the same tiles [r C, (r + 1) C) of its state
+    // (rows = 2^(n-16), the layout of launch_group_histogram), whatever the state's place in the
+    // batch.  Within a chunk the bins accumulate per warp in shared memory in a fixed order.
+    const bool hist = hist_mask != 0 && __builtin_popcount(hist_mask) <= kGroupMaxBits;
+    const int hist_bins = hist ? 1 << __builtin_popcount(hist_mask) : 0;
+    const int chunk = hist ? (qubits > 16 ? 1 << (16 - p.k) : 1 << (qubits - p.k)) : 1;
+    const int warps = nt / 32;
+    const size_t hist_bytes = hist ? sizeof(double) * (size_t)warps * hist_bins : 0;
+    const bool large = !tabled && !hist && qubits >= 26;
     const bool second = large && !fp64 && 2 * tile_bytes + prog_bytes <= (100u << 10);
     // Complex128: the exchange tile itself takes the next item's copy once the pass's last
     // exchange is done, so the copy overlaps the ops after it, the flush and the stores.
@@ -899,8 +909,10 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int
     os << "V* tile = reinterpret_cast<V*>(smem_raw);\n";
     if (second) os << "V* ptile = reinterpret_cast<V*>(smem_raw + " << tile_bytes << ");\n";
     if (late) os << "V* ptile = tile;\n";
-    os << "FusedOp* prog = reinterpret_cast<FusedOp*>(smem_raw + " << tiles * tile_bytes << ");\n";
-    os << "double* table = reinterpret_cast<double*>(smem_raw + " << (tiles * tile_bytes + prog_bytes) << ");\n";
+    if (hist) os << "double* hacc = reinterpret_cast<double*>(smem_raw + " << tiles * tile_bytes << ");\n";
+    os << "FusedOp* prog = reinterpret_cast<FusedOp*>(smem_raw + " << tiles * tile_bytes + hist_bytes << ");\n";
+    os << "double* table = reinterpret_cast<double*>(smem_raw + " << (tiles * tile_bytes + hist_bytes + prog_bytes)
+       << ");\n";
     os << "const u32 t = threadIdx.x;\n";
     os << "{ const uint2* src = reinterpret_cast<const uint2*>(P.ops); uint2* dst = reinterpret_cast<uint2*>(prog);\n"
        << "  for (int i = t; i < " << p.op_count * (int)(sizeof(FusedOp) / 8) << "; i += " << nt
@@ -933,7 +945,13 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int
     };
     prefetch("(long long)blockIdx.x");
     os << "int current = -1;\n";
-    os << "for (long long item = blockIdx.x; item < total; item += gridDim.x) {\n";
+    if (hist) {
+        os << "for (long long u = blockIdx.x; u < total / " << chunk << "; u += gridDim.x) {\n";
+        os << "for (int i = t; i < " << warps * hist_bins << "; i += " << nt << ") hacc[i] = 0.0;\n";
+        os << "for (int cc = 0; cc < " << chunk << "; ++cc) {\nconst long long item = u * " << chunk << " + cc;\n";
+    } else {
+        os << "for (long long item = blockIdx.x; item < total; item += gridDim.x) {\n";
+    }
     os << "const int b = (int)(item >> P.cta_shift);\nconst u32 cta = (u32)item & cta_mask;\n";
     if (piped) os << "asm volatile(\"cp.async.wait_group 0;\" ::: \"memory\");\n";
     os << "__syncthreads();\n";
@@ -1004,6 +1022,53 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int
             carry->g = cplx(1.0, 0.0);
         }
     }
+    if (hist) {
+        // bin bit j is the j-th group qubit; in the store layout each is a register bit, a
+        // thread bit (a lane bit when below 5) or a qubit outside the block
+        uint32_t reg_gm = 0, lane_gm = 0;
+        int reg_bin[R] = {};
+        std::string rt = "0u";
+        int tb = 0;
+        std::vector<int> thread_rank((size_t)p.k, -1);
+        for (int b = 0; b < p.k; ++b)
+            if (!(g.regmask() & (1u << b))) thread_rank[(size_t)b] = tb++;
+        int j = 0;
+        for (int q = 0; q < qubits; ++q) {
+            if (!(hist_mask & (1u << q))) continue;
+            int lb = -1;
+            for (int b = 0; b < p.k; ++b)
+                if (p.q[b] == q) lb = b;
+            if (lb < 0) {
+                rt += " | (((outer >> " + std::to_string(q) + ") & 1u) << " + std::to_string(j) + ")";
+            } else if (g.reg_of_local(lb) >= 0) {
+                const int m = g.reg_of_local(lb);
+                reg_gm |= 1u << m;
+                reg_bin[m] = j;
+            } else {
+                const int r = thread_rank[(size_t)lb];
+                rt += " | (((t >> " + std::to_string(r) + ") & 1u) << " + std::to_string(j) + ")";
+                if (r < 5) lane_gm |= 1u << r;
+            }
+            ++j;
+        }
+        os << "{ const u32 hb = " << rt << ";\n";
+        os << "const bool hw = (t & " << hexu(~lane_gm & 31u) << ") == 0u;\nconst int hwarp = (int)(t >> 5);\n";
+        for (uint32_t pat = 0; pat < (uint32_t)NR; ++pat) {
+            if ((pat & ~reg_gm) != 0) continue;
+            uint32_t bin = 0;
+            for (int m = 0; m < R; ++m)
+                if ((pat >> m) & 1u) bin |= 1u << reg_bin[m];
+            os << "{ double v = 0.0;\n";
+            for (int i = 0; i < NR; ++i)
+                if (((uint32_t)i & reg_gm) == pat)
+                    os << "v += (double)" << g.X(i) << " * " << g.X(i) << " + (double)" << g.Y(i) << " * " << g.Y(i)
+                       << ";\n";
+            for (int l = 0; l < 5; ++l)
+                if (!((lane_gm >> l) & 1u)) os << "v += __shfl_xor_sync(0xffffffffu, v, " << (1 << l) << ");\n";
+            os << "if (hw) hacc[hwarp * " << hist_bins << " + (hb | " << hexu(bin) << ")] += v; }\n";
+        }
+        os << "}\n";
+    }
     os << "{ const u32 g1 = outer | " << deposit_expr("t", thread_out) << ";\n";
     for (int i = 0; i < NR; ++i) {
         uint32_t gi = 0;
@@ -1011,7 +1076,15 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int
             if ((i >> m) & 1) gi |= reg_out_g[m];
         os << "{ V v; v.x = " << g.X(i) << "; v.y = " << g.Y(i) << "; s[g1 | " << hexu(gi) << "] = v; }\n";
     }
-    os << "}\n(void)base;\n}\n}\n";
+    os << "}\n(void)base;\n}\n";
+    if (hist) {
+        os << "__syncthreads();\n";
+        os << "for (int k = t; k < " << hist_bins << "; k += " << nt << ") { double sum = 0.0;\n"
+           << "  for (int w = 0; w < " << warps << "; ++w) sum += hacc[w * " << hist_bins << " + k];\n"
+           << "  hist[u * " << hist_bins << " + k] = sum; }\n";
+        os << "__syncthreads();\n}\n";
+    }
+    os << "}\n";
 
     std::ostringstream hd;
     hd << kPrelude;
@@ -1025,12 +1098,14 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int
     const size_t na = std::max<size_t>(1, g.aux.size());
     hd << "struct Aux { " << g.T << " v[" << na << "]; };\n";
     hd << "extern \"C\" __global__ void __launch_bounds__(" << nt << ", " << minb
-       << ") qm_pass(V* __restrict__ s0, const __grid_constant__ FusedLaunch P, const __grid_constant__ Aux A) {\n";
+       << ") qm_pass(V* __restrict__ s0, const __grid_constant__ FusedLaunch P, const __grid_constant__ Aux A"
+       << (hist ? ", double* __restrict__ hist" : "") << ") {\n";
     Generated out;
     // the constants travel as a kernel parameter (at most 32764 bytes with the launch record)
     if (g.aux.size() > kMaxAuxValues + 1000) return out;
     out.src = hd.str() + os.str();
     out.tiles = tiles;
+    out.hist_bins = hist_bins;
     if (fp64) {
         std::vector<double> v(na, 0.0);
         std::copy(g.aux.begin(), g.aux.end(), v.begin());
@@ -1054,7 +1129,7 @@ std::vector<Generated> generate_plan(const Plan& plan, bool chained) {
     Carry carry;
     for (size_t i = 0; i < plan.passes.size(); ++i)
         out.push_back(generate(plan.passes[i], plan.ops, plan.qubits, fp64, chained ? &carry : nullptr,
-                               i + 1 == plan.passes.size()));
+                               i + 1 == plan.passes.size(), i + 1 == plan.passes.size() ? plan.hist_mask : 0u));
     return out;
 }
 
@@ -1166,8 +1241,10 @@ void install(Plan& plan, std::vector<Generated>& gen, bool cached_only) {
         if (k) {
             plan.jit_aux[i] = std::move(gen[i].aux);
             plan.jit_tiles[i] = gen[i].tiles;
+            plan.jit_hist_bins[i] = gen[i].hist_bins;
         }
     }
+    plan.hist_fused = !gen.empty() && plan.jit.back() && gen.back().hist_bins > 0;
 }
 
 bool all_cached(const std::vector<Generated>& gen) {
@@ -1188,6 +1265,8 @@ void jit_prepare(Plan& plan) {
     plan.jit.assign(plan.passes.size(), nullptr);
     plan.jit_aux.assign(plan.passes.size(), {});
     plan.jit_tiles.assign(plan.passes.size(), 1);
+    plan.jit_hist_bins.assign(plan.passes.size(), 0);
+    plan.hist_fused = false;
     if (!jit_enabled() || plan.passes.empty()) return;
     std::vector<Generated> gen = generate_plan(plan, true);
     if (compile_all(gen)) {
@@ -1203,6 +1282,8 @@ void jit_lookup(Plan& plan) {
     plan.jit.assign(plan.passes.size(), nullptr);
     plan.jit_aux.assign(plan.passes.size(), {});
     plan.jit_tiles.assign(plan.passes.size(), 1);
+    plan.jit_hist_bins.assign(plan.passes.size(), 0);
+    plan.hist_fused = false;
     if (!jit_enabled() || plan.passes.empty()) return;
     {
         std::lock_guard<std::mutex> lock(g_cache_mu);
@@ -1227,7 +1308,10 @@ cudaError_t launch_plan_pass(const Plan& plan, size_t pass, void* amps, const Fu
     if (batch && (batch->states < 1 || batch->states > 65535)) return cudaErrorInvalidValue;
     FusedLaunch L = fused_launch_params(plan.qubits, p, plan.d_ops, batch);
     const bool fp64 = plan.precision != QM_FP32;
+    const int hist_bins = pass < plan.jit_hist_bins.size() ? plan.jit_hist_bins[pass] : 0;
+    if (hist_bins > 0 && (!batch || !batch->hist)) return cudaErrorInvalidValue;
     const size_t smem = ((size_t)(fp64 ? 16 : 8) * (size_t)plan.jit_tiles[pass] << p.k) +
+                        sizeof(double) * (size_t)((1 << (p.k - R)) / 32) * (size_t)hist_bins +
                         (((size_t)p.op_count * sizeof(FusedOp) + 15) & ~size_t(15)) +
                         sizeof(double) * 8 * (size_t)L.table_slots;
     static const int sms = [] {
@@ -1242,10 +1326,13 @@ cudaError_t launch_plan_pass(const Plan& plan, size_t pass, void* amps, const Fu
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
-    const int64_t items = (int64_t)L.states << L.cta_shift;
+    int64_t items = (int64_t)L.states << L.cta_shift;
+    if (hist_bins > 0)  // work units are chunks of tiles (the joint-mass partial rows)
+        items = (int64_t)L.states * (plan.qubits > 16 ? (int64_t)1 << (plan.qubits - 16) : 1);
     const int64_t grid = std::min<int64_t>(items, (int64_t)sms * per_sm);
     void* arg0 = amps;
-    void* args[] = {&arg0, &L, const_cast<unsigned char*>(plan.jit_aux[pass].data())};
+    double* hist = batch ? batch->hist : nullptr;
+    void* args[] = {&arg0, &L, const_cast<unsigned char*>(plan.jit_aux[pass].data()), &hist};
     e = cudaLaunchKernel(kernel, dim3((unsigned)grid), dim3((unsigned)threads), args, smem, st);
     if (e == cudaSuccess) ++g_launches;
     return e;

@@ -377,6 +377,9 @@ extern "C" int32_t qm_trajectories_run(qm_context* ctx, int32_t qubits, int32_t 
         QM_CUDA(cudaMemcpyAsync(d_decisions, P.all_decisions.data(), sizeof(Decision) * P.all_decisions.size(),
                                 cudaMemcpyHostToDevice, st));
     for (Segment& s : P.segments) {
+        // a segment followed by a damping group computes the group's joint masses in the
+        // epilogue of its last pass when that pass compiles
+        if (s.group >= 0 && !s.plan.passes.empty()) s.plan.hist_mask = P.groups[(size_t)s.group];
         jit_prepare(s.plan);  // layers repeat: most segments share compiled passes
         rc = plan_upload(s.plan, st);
         if (rc) return rc;
@@ -426,9 +429,10 @@ extern "C" int32_t qm_trajectories_run(qm_context* ctx, int32_t qubits, int32_t 
             QM_CUDA(launch_decide(da, Bw, st));
             for (size_t p = 0; p < s.plan.passes.size(); ++p) {
                 FusedBatch fb{Bw, 1ull << n, table, table_stride, s.pass_first[p], s.pass_count[p]};
+                fb.hist = partials;
                 QM_CUDA(launch_plan_pass(s.plan, p, amps, &fb, st));
             }
-            if (s.group >= 0)
+            if (s.group >= 0 && !s.plan.hist_fused)
                 QM_CUDA(launch_group_histogram(amps, n, precision, Bw, P.groups[(size_t)s.group], partials, st));
             prev_group = s.group;
         }
