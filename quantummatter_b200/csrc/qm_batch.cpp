@@ -476,7 +476,8 @@ int32_t vqe_evaluate(qm_context* ctx, int32_t qubits, int32_t precision, const q
         ~Release() { plan_release(p); }
     } release{plan};
     {
-        jit_prepare(plan);  // one structure for every circuit of every wave
+        plan.start_zero = true;  // every circuit starts from |0...0>
+        jit_prepare(plan);       // one structure for every circuit of every wave
         int32_t urc = plan_upload(plan, ctx->stream);
         if (urc) return urc;
     }
@@ -568,7 +569,7 @@ int32_t vqe_evaluate(qm_context* ctx, int32_t qubits, int32_t precision, const q
     auto enqueue_wave = [&](int buf, int count) -> int32_t {
         QM_CUDA(cudaMemcpyAsync(batch->table, h_table[buf], sizeof(double) * (size_t)count * slot_count * 8,
                                 cudaMemcpyHostToDevice, st));
-        QM_CUDA(launch_reset_batched(batch->amps, qubits, precision, count, st));
+        if (!plan.zero_fused) QM_CUDA(launch_reset_batched(batch->amps, qubits, precision, count, st));
         int32_t r2 = enqueue_plan(batch, plan, count, batch->table, (size_t)slot_count * 8, st);
         if (r2) return r2;
         r2 = enqueue_tiles(batch, tp, count, st);

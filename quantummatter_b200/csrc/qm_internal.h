@@ -117,6 +117,11 @@ struct Plan {
     // (hist_fused), in the layout of launch_group_histogram.
     uint32_t hist_mask = 0;
     bool hist_fused = false;
+    // Every state starts the plan as |0...0> (the batched variational evaluator): the first pass
+    // writes that state into its registers instead of loading it when it compiles (zero_fused),
+    // so the caller's reset can be skipped.
+    bool start_zero = false;
+    bool zero_fused = false;
     bool borrowed = false;          // d_ops belongs to a context buffer
     int64_t planned_bytes = 0;
     int32_t launches = 0;

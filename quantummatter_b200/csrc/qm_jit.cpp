@@ -836,10 +836,11 @@ struct Generated {
     std::vector<unsigned char> aux;  // the parameter block: doubles (complex128) or floats
     int tiles = 1;                   // tiles of shared memory (2: pipelined)
     int hist_bins = 0;               // joint-mass epilogue bins (0: none)
+    bool zero_start = false;         // the pass writes |0...0> instead of loading the state
 };
 
 Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int qubits, bool fp64, Carry* carry,
-                   bool last, uint32_t hist_mask = 0) {
+                   bool last, uint32_t hist_mask = 0, bool zero_start = false) {
     Gen g;
     g.fp64 = fp64;
     g.K = p.k;
@@ -889,7 +890,7 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int
     const int chunk = hist ? (qubits > 16 ? 1 << (16 - p.k) : 1 << (qubits - p.k)) : 1;
     const int warps = nt / 32;
     const size_t hist_bytes = hist ? sizeof(double) * (size_t)warps * hist_bins : 0;
-    const bool large = !tabled && !hist && qubits >= 26;
+    const bool large = !tabled && !hist && !zero_start && qubits >= 26;
     const bool second = large && !fp64 && 2 * tile_bytes + prog_bytes <= (100u << 10);
     // Complex128: the exchange tile itself takes the next item's copy once the pass's last
     // exchange is done, so the copy overlaps the ops after it, the flush and the stores.
@@ -981,7 +982,11 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int
             uint32_t gi = 0;
             for (int m = 0; m < R; ++m)
                 if ((i >> m) & 1) gi |= reg_in_g[m];
-            os << "{ const V v = s[g0 | " << hexu(gi) << "]; x" << i << " = v.x; y" << i << " = v.y; }\n";
+            if (zero_start)  // |0...0>: amplitude 1 at index 0 of every state, nothing read
+                os << "x" << i << " = (g0 | " << hexu(gi) << ") == 0u ? (" << g.T << ")1 : (" << g.T << ")0; y" << i
+                   << " = (" << g.T << ")0;\n";
+            else
+                os << "{ const V v = s[g0 | " << hexu(gi) << "]; x" << i << " = v.x; y" << i << " = v.y; }\n";
         }
         os << "}\n";
         os << "u32 base = " << g.base_expr() << ";\n";
@@ -1106,6 +1111,7 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int
     out.src = hd.str() + os.str();
     out.tiles = tiles;
     out.hist_bins = hist_bins;
+    out.zero_start = zero_start;
     if (fp64) {
         std::vector<double> v(na, 0.0);
         std::copy(g.aux.begin(), g.aux.end(), v.begin());
@@ -1129,7 +1135,8 @@ std::vector<Generated> generate_plan(const Plan& plan, bool chained) {
     Carry carry;
     for (size_t i = 0; i < plan.passes.size(); ++i)
         out.push_back(generate(plan.passes[i], plan.ops, plan.qubits, fp64, chained ? &carry : nullptr,
-                               i + 1 == plan.passes.size(), i + 1 == plan.passes.size() ? plan.hist_mask : 0u));
+                               i + 1 == plan.passes.size(), i + 1 == plan.passes.size() ? plan.hist_mask : 0u,
+                               i == 0 && plan.start_zero));
     return out;
 }
 
@@ -1245,6 +1252,7 @@ void install(Plan& plan, std::vector<Generated>& gen, bool cached_only) {
         }
     }
     plan.hist_fused = !gen.empty() && plan.jit.back() && gen.back().hist_bins > 0;
+    plan.zero_fused = !gen.empty() && plan.jit.front() && gen.front().zero_start;
 }
 
 bool all_cached(const std::vector<Generated>& gen) {
@@ -1267,6 +1275,7 @@ void jit_prepare(Plan& plan) {
     plan.jit_tiles.assign(plan.passes.size(), 1);
     plan.jit_hist_bins.assign(plan.passes.size(), 0);
     plan.hist_fused = false;
+    plan.zero_fused = false;
     if (!jit_enabled() || plan.passes.empty()) return;
     std::vector<Generated> gen = generate_plan(plan, true);
     if (compile_all(gen)) {
@@ -1284,6 +1293,7 @@ void jit_lookup(Plan& plan) {
     plan.jit_tiles.assign(plan.passes.size(), 1);
     plan.jit_hist_bins.assign(plan.passes.size(), 0);
     plan.hist_fused = false;
+    plan.zero_fused = false;
     if (!jit_enabled() || plan.passes.empty()) return;
     {
         std::lock_guard<std::mutex> lock(g_cache_mu);
