@@ -1010,7 +1010,10 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int
         g.op(o, op);
     }
     if (carry && !last) {
-        g.rescale();
+        // |g m| <= 1 per rotation, so the stored amplitudes grow by 1 / |G| until a rescale;
+        // rescaling once |G| falls below 1e-60 (complex128) or 1e-9 (complex64) keeps them far
+        // from overflow and saves a multiply per amplitude in most passes
+        if (std::abs(g.G) < (fp64 ? 1e-60 : 1e-9)) g.rescale();
         g.normalize();
         carry->pend.clear();
         for (const Pend& e : g.pend) {
