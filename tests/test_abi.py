@@ -39,6 +39,23 @@ def test_library_exports_every_declared_entry_point():
     assert limit and int(limit.group(1)) == _lib.NOALLOC_MAX_TERMS
 
 
+def test_shipped_abi_inventory_matches_the_header():
+    """include/qm_b200.shipped.txt is the shipped surface (prototypes, struct fields, defines),
+    as PublicAPI.Shipped.txt is for the reference's assemblies: changing the header without it
+    fails here.  Regenerate with `python include/shipped_abi.py --write` and, for a change that
+    breaks callers, raise QM_ABI_VERSION."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("shipped_abi", ROOT / "include" / "shipped_abi.py")
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    want = (ROOT / "include" / "qm_b200.shipped.txt").read_text().splitlines()
+    got = mod.inventory(HEADER.read_text())
+    added, removed = sorted(set(got) - set(want)), sorted(set(want) - set(got))
+    assert not added and not removed, {"not in the inventory": added, "gone from the header": removed}
+    functions = {re.search(r"\b(qm_\w+)\(", line).group(1) for line in got if line.startswith("function ")}
+    assert functions == declared_symbols()
+
+
 def test_struct_layouts_match_the_header():
     assert C.sizeof(_lib.Operation) == 88
     assert C.sizeof(_lib.Gate) == 80
