@@ -199,7 +199,8 @@ def run_vqe(args) -> None:
     from quantummatter_b200.variational import B200VariationalEnergyEvaluator
     from quantummatter_b200.workloads import hardware_efficient_ansatz, uniform_parameters, xxz_chain
     sizes = [int(s) for s in args.sizes.split(",")]
-    ctx = B200Context(B200BackendOptions(DeviceMemoryBudgetBytes=120 << 30, StagingMemoryBudgetBytes=1 << 30))
+    ctx = B200Context(B200BackendOptions(DeviceMemoryBudgetBytes=120 << 30, StagingMemoryBudgetBytes=1 << 30,
+                                         FusionWidth=args.width))
     results = {}
     total_circuits = 0
     max_de = 0.0
