@@ -323,3 +323,31 @@ def test_30_qubit_brick_round_trip_and_norm(gpu_context):
         b.Evolve(c, fusion_width=1)
         diff = np.max(np.abs(a.Download() - b.Download()))
     assert diff <= 1e-12
+
+
+def test_30_qubit_brick_round_trip_through_compiled_plans(gpu_context):
+    """The headline path at its own size: the 30-qubit brick and its inverse as plans, whose passes
+    are compiled for their op sequence (rotations between deferred phases, phases carried from
+    pass to pass, the next tile copied during the last exchange).  The round trip returns |0...0>
+    and the norm stays 1 after the forward circuit."""
+    from quantummatter_b200.backend import Plan, jit_info
+    from test_oracle_pinning import _inverse
+    c = brick_circuit(30, 40)
+    before = jit_info()
+    fwd, back = Plan(gpu_context, c, FP64), Plan(gpu_context, _inverse(c), FP64)
+    try:
+        with DeviceState(gpu_context, 30, FP64) as st:
+            fwd.execute(st)
+            _, mass = st.ExpectationValues([])
+            assert abs(mass - 1) <= 1e-11
+            back.execute(st)
+            vals, mass = st.ExpectationValues([PauliString("Z" * 30)])
+            assert abs(vals[0] - 1) <= 1e-10 and abs(mass - 1) <= 1e-11
+            m0, _ = st.QubitMasses(0)
+            assert abs(m0 - 1) <= 1e-10
+    finally:
+        fwd.Dispose()
+        back.Dispose()
+    after = jit_info()
+    if before["available"]:
+        assert after["failed"] == before["failed"] and after["launches"] > before["launches"]
