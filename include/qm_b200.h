@@ -248,6 +248,10 @@ int32_t qm_plan_program(int32_t qubits, int32_t precision, const qm_gate* gates,
 int32_t qm_jit_info(int32_t* available, int64_t* kernels, int64_t* failed, int64_t* launches);
 int32_t qm_jit_source(int32_t qubits, int32_t precision, const qm_gate* gates, int32_t count,
                       int32_t fusion_width, int32_t pass, char* buffer, size_t size, size_t* length);
+/* The constant parameter block that the same compiled pass is launched with (the rotation and
+ * phase constants of its kernel parameter `A`), as bytes; for inspection and tests. */
+int32_t qm_jit_constants(int32_t qubits, int32_t precision, const qm_gate* gates, int32_t count,
+                         int32_t fusion_width, int32_t pass, void* buffer, size_t size, size_t* length);
 
 /* ---------------------------------------------------------------- noise primitives */
 

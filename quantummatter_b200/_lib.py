@@ -152,6 +152,8 @@ SIGNATURES = {
     "qm_jit_info": (I32, [I32P, I64P, I64P, I64P]),
     "qm_jit_source": (I32, [I32, I32, C.POINTER(Gate), I32, I32, I32, C.c_char_p, C.c_size_t,
                             C.POINTER(C.c_size_t)]),
+    "qm_jit_constants": (I32, [I32, I32, C.POINTER(Gate), I32, I32, I32, C.c_void_p, C.c_size_t,
+                               C.POINTER(C.c_size_t)]),
     "qm_state_noise_apply": (I32, [P, I32, C.c_double, I32, NEXT_DOUBLE_FN, P]),
     "qm_jit_expect_source": (I32, [I32, I32, C.POINTER(PauliTermC), I32, I32, C.c_char_p, C.c_size_t,
                                    C.POINTER(C.c_size_t)]),

@@ -1614,6 +1614,23 @@ extern "C" int32_t qm_jit_info(int32_t* available, int64_t* kernels, int64_t* fa
 }
 
 // Source of the compiled kernel of one pass of a plan made for these gates (inspection and tests).
+// The constant parameter block (kernel parameter A) of the same pass, as bytes.
+extern "C" int32_t qm_jit_constants(int32_t qubits, int32_t precision, const qm_gate* gates, int32_t count,
+                                    int32_t fusion_width, int32_t pass, void* buffer, size_t size, size_t* length) {
+    using namespace qm;
+    int32_t rc = validate_prepared_gates(gates, count, qubits);
+    if (rc) return rc;
+    Plan plan;
+    std::string err;
+    std::vector<qm_gate> list(gates, gates + count);
+    if (!plan_fused(list, qubits, precision, fusion_width, plan, err)) return fail(QM_E_ARG, "planner: " + err);
+    if (pass < 0 || (size_t)pass >= plan.passes.size()) return fail(QM_E_RANGE, "pass index out of range");
+    const std::vector<unsigned char> aux = generate_plan(plan, true)[(size_t)pass].aux;
+    if (length) *length = aux.size();
+    if (buffer && size) std::memcpy(buffer, aux.data(), std::min(size, aux.size()));
+    return QM_OK;
+}
+
 extern "C" int32_t qm_jit_source(int32_t qubits, int32_t precision, const qm_gate* gates, int32_t count,
                                  int32_t fusion_width, int32_t pass, char* buffer, size_t size, size_t* length) {
     using namespace qm;

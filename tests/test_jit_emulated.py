@@ -1,0 +1,62 @@
+"""Compiled passes run on the CPU (tests/jit_emulator.*) against the oracle.
+
+The generated source of every pass of a plan is built with g++ and run as C++, chained as the
+library chains it, so the deferred-phase algebra (rotations between pending phases, phases
+rewritten by X, CNOT and SWAP, resolved before controlled ops and Toffolis, carried across
+passes and flushed by the last one) is checked here without a GPU, on circuits that reach each
+of those paths.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+
+import jit_emulator as je
+import oracle as orc
+from circuits import random_circuit, random_state
+from quantummatter_b200.algorithms import QuantumFourierTransform
+from quantummatter_b200.backend import FP32, FP64
+from quantummatter_b200.circuit import QuantumCircuit, u3
+from quantummatter_b200.workloads import SplitMix64, brick_circuit
+from test_abi import diagonal_heavy_circuit
+
+pytestmark = pytest.mark.skipif(not je.available(), reason="g++ not found")
+
+
+def frame_mix(n: int, layers: int, seed: int) -> QuantumCircuit:
+    """U3 layers with X, CNOT (register and thread controls), SWAP, CZ, Ry and H in between:
+    pending phases get conjugated, moved between sets and resolved."""
+    rng = SplitMix64(seed)
+    c = QuantumCircuit(n)
+    for layer in range(layers):
+        for q in range(n):
+            c.U(q, u3(rng.uniform(0, 6.3), rng.uniform(0, 6.3), rng.uniform(0, 6.3)))
+        c.X(layer % n).CNot((layer + 3) % n, (layer + 1) % n).Swap(layer % n, (layer + 5) % n)
+        c.CZ(1, n - 2).Ry((layer + 2) % n, rng.uniform(0, 6.3)).H((layer + 4) % n)
+        if n > 3:
+            c.Toffoli(0, 1, n - 1)
+        for q in range(layer % 2, n - 1, 2):
+            c.CNot(q, q + 1)
+    return c
+
+
+CASES = [
+    ("brick_fp64", lambda: brick_circuit(14, 10, seed=8), FP64, 1e-12),
+    ("brick_fp32", lambda: brick_circuit(14, 10, seed=9), FP32, 2e-5),
+    ("frame_mix", lambda: frame_mix(13, 5, 11), FP64, 1e-12),
+    ("random", lambda: random_circuit(12, 250, seed=21), FP64, 1e-12),
+    ("diagonal", lambda: diagonal_heavy_circuit(12, 250, seed=22), FP64, 1e-12),
+    ("qft", lambda: QuantumFourierTransform.CreateCircuit(13), FP64, 1e-12),
+]
+
+
+@pytest.mark.parametrize("name,make,precision,tol", CASES, ids=[c[0] for c in CASES])
+def test_compiled_passes_on_the_cpu_match_the_oracle(name, make, precision, tol):
+    c = make()
+    psi = random_state(c.QubitCount, 3)
+    want = orc.execute(c, psi)
+    got = je.run_plan(c, precision, psi)
+    assert np.max(np.abs(got - want)) <= tol
+    assert abs(np.linalg.norm(got) - math.sqrt(np.vdot(psi, psi).real)) <= 100 * tol
