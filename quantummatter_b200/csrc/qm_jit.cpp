@@ -3,16 +3,23 @@
 // k_fused interprets a pass program: for every op it decodes the record, selects the register
 // bit through a switch and, for an X or SWAP on register bits, moves the amplitudes between
 // registers.  Here a pass's op sequence is turned into straight-line CUDA C++ and compiled once
-// with NVRTC for sm_100a.  The generated kernel takes the same parameters and shared-memory
-// layout as k_fused (the program is still staged, and every coefficient is still read from it
-// or from the batch table), so one compiled kernel serves every pass with the same structure
-// whatever its angles.  What the generation fixes at compile time:
+// with NVRTC for sm_100a.  The generated kernel takes k_fused's launch record and shared-memory
+// layout plus a constant parameter block: coefficients come from the staged program, the batch
+// table or that block, never from the source, so one compiled kernel serves every pass with
+// the same structure and rotation forms.  What the generation fixes at compile time:
 //   - the register of every op, and the register pairs it touches;
 //   - the control predicates: register bits select pairs at compile time, thread bits become
 //     one uniform test per op, bits outside the block one test per work item;
 //   - an X, CNOT or SWAP acting on register bits only renames registers: no instruction;
-//   - the load, store and shared-memory exchange addresses as constants and bit deposits.
-// NVRTC is loaded at run time; without it every pass runs on k_fused, the GPU interpreter.
+//   - the load, store and shared-memory exchange addresses as constants and bit deposits;
+//   - uncontrolled 2x2 unitaries as scaled rotations between deferred phases (below), with the
+//     phases carried from pass to pass of a plan;
+//   - from 26 qubits, the copy of the next work item's tile during the current one;
+//   - the variants of the batch workloads: a first pass that starts from |0...0>, a last pass
+//     whose epilogue writes a damping group's joint masses.
+// The tiled expectation of the batched variational evaluator is generated here as well, for its
+// term list.  NVRTC is loaded at run time; without it every pass runs on k_fused, the GPU
+// interpreter, and every expectation on the generic tiled kernel.
 #include <cuda_runtime.h>
 #include <dlfcn.h>
 #include <nvrtc.h>
