@@ -410,6 +410,7 @@ extern "C" int32_t qm_context_destroy(qm_context* ctx) {
         if (ctx->host_scratch) cudaFreeHost(ctx->host_scratch);
         if (ctx->staging) cudaFree(ctx->staging);
         if (ctx->program) cudaFree(ctx->program);
+        release_bounce(ctx);
         if (ctx->ev_start) cudaEventDestroy(ctx->ev_start);
         if (ctx->ev_stop) cudaEventDestroy(ctx->ev_stop);
         if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -504,7 +505,7 @@ extern "C" int32_t qm_execute_host(qm_context* ctx, int32_t qubits, const qm_ope
         cudaEventCreate(&t0); cudaEventCreate(&t1); cudaEventCreate(&t2); cudaEventCreate(&t3);
         cudaEventRecord(t0, ctx->stream);
     }
-    cudaError_t e = cudaMemcpyAsync(dev, amps, (size_t)bytes, cudaMemcpyHostToDevice, ctx->stream);
+    cudaError_t e = host_to_device(ctx, dev, amps, (size_t)bytes);
     if (e == cudaSuccess && profile) cudaEventRecord(t1, ctx->stream);
     if (e == cudaSuccess) rc = run_plan(ctx, plan, dev, cancel);
     if (e == cudaSuccess && rc == QM_OK) {
@@ -514,7 +515,7 @@ extern "C" int32_t qm_execute_host(qm_context* ctx, int32_t qubits, const qm_ope
     if (e == cudaSuccess && rc == QM_OK && cancelled(cancel)) rc = fail(QM_E_CANCELLED, "operation cancelled");
     // commit: only after every launch completed and the last cancellation check passed
     if (e == cudaSuccess && rc == QM_OK) {
-        e = cudaMemcpyAsync(amps, dev, (size_t)bytes, cudaMemcpyDeviceToHost, ctx->stream);
+        e = device_to_host(ctx, amps, dev, (size_t)bytes);
         if (e == cudaSuccess && profile) cudaEventRecord(t3, ctx->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     }
@@ -626,7 +627,7 @@ extern "C" int32_t qm_noise_apply_host(qm_context* ctx, int32_t kind, double p, 
     void* dev = nullptr;
     int32_t rc = device_buffer(ctx, (size_t)bytes, &dev);
     if (rc) return rc;
-    QM_CUDA(cudaMemcpyAsync(dev, amps, (size_t)bytes, cudaMemcpyHostToDevice, ctx->stream));
+    QM_CUDA(host_to_device(ctx, dev, amps, (size_t)bytes));
     if (kind == 3) {
         double m0 = 0, m1 = 0;
         rc = device_masses(ctx, dev, qubits, QM_FP64, target, &m0, &m1);
@@ -640,7 +641,7 @@ extern "C" int32_t qm_noise_apply_host(qm_context* ctx, int32_t kind, double p, 
         QM_CUDA(launch_pauli(dev, qubits, QM_FP64, target, b.pauli, ctx->stream));
     }
     QM_CUDA(cudaStreamSynchronize(ctx->stream));
-    QM_CUDA(cudaMemcpyAsync(amps, dev, (size_t)bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    QM_CUDA(device_to_host(ctx, amps, dev, (size_t)bytes));
     QM_CUDA(cudaStreamSynchronize(ctx->stream));
     return QM_OK;
 }
@@ -715,7 +716,7 @@ extern "C" int32_t qm_state_upload(qm_state* st, const double* amps, int64_t len
     std::lock_guard<std::recursive_mutex> lock(ctx->mu);
     QM_CUDA(cudaSetDevice(ctx->device));
     if (st->precision == QM_FP64) {
-        QM_CUDA(cudaMemcpyAsync(st->amps, amps, (size_t)(16 * length), cudaMemcpyHostToDevice, ctx->stream));
+        QM_CUDA(host_to_device(ctx, st->amps, amps, (size_t)(16 * length)));
     } else {
         const int64_t chunk = int64_t(1) << 21;  // amplitudes per staging chunk (32 MiB FP64)
         rc = ensure_scratch(ctx, (size_t)(16 * std::min(chunk, length)));
@@ -739,7 +740,7 @@ extern "C" int32_t qm_state_download(qm_state* st, double* amps, int64_t length)
     std::lock_guard<std::recursive_mutex> lock(ctx->mu);
     QM_CUDA(cudaSetDevice(ctx->device));
     if (st->precision == QM_FP64) {
-        QM_CUDA(cudaMemcpyAsync(amps, st->amps, (size_t)(16 * length), cudaMemcpyDeviceToHost, ctx->stream));
+        QM_CUDA(device_to_host(ctx, amps, st->amps, (size_t)(16 * length)));
     } else {
         const int64_t chunk = int64_t(1) << 21;
         rc = ensure_scratch(ctx, (size_t)(16 * std::min(chunk, length)));

@@ -366,7 +366,16 @@ struct qm_context {
     // device copy of the op program of one-shot executions (reused, grows as needed)
     void* program = nullptr;
     size_t program_bytes = 0;
+    // page-locked bounce buffers of whole-state copies from pageable host memory (qm_transfer.cpp)
+    void* bounce[2] = {nullptr, nullptr};
+    cudaEvent_t bounce_done[2] = {nullptr, nullptr};
 };
+// Whole-state copies with a caller's host buffer on the context's stream (qm_transfer.cpp):
+// host_to_device returns once the host buffer has been read (the device copy may still be in
+// flight on the stream); device_to_host returns once the host buffer holds the data.
+cudaError_t host_to_device(qm_context* ctx, void* dev, const void* host, size_t bytes);
+cudaError_t device_to_host(qm_context* ctx, void* host, const void* dev, size_t bytes);
+void release_bounce(qm_context* ctx);
 
 struct qm_state {
     qm_context* ctx = nullptr;

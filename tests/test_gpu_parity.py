@@ -301,6 +301,37 @@ def test_measure_all_collapses_like_the_oracle(gpu_context):
         assert np.array_equal(got, want_state)
 
 
+@pytest.mark.parametrize("n", [21, 24])
+def test_pageable_host_buffers_match_page_locked_ones(gpu_context, n):
+    """Whole-state copies from pageable host memory of 16 MiB and more move through the
+    context's page-locked bounce buffers (one partial 64 MiB chunk at 21 qubits, four at 24);
+    the results are bit-identical to the same calls on a page-locked buffer, for the drop-in
+    port, the noise port and a device state's upload and download."""
+    from quantummatter_b200.noise import NoiseChannel
+    psi = random_state(n, 90 + n)
+    circuit = brick_circuit(n, 2, seed=n)
+    backend = B200StateVectorBackend(context=gpu_context)
+    noise = B200NoiseChannelBackend(context=gpu_context)
+    pinned = gpu_context.host_array(1 << n)
+    try:
+        results = []
+        for buffer in (pinned.array, np.empty(1 << n, dtype=np.complex128)):
+            buffer[:] = psi
+            backend.Execute(circuit, buffer)
+            noise.Apply(NoiseChannel(3, 0.37), n - 1, buffer, FixedRandom(0.5))
+            with DeviceState(gpu_context, n, FP64) as st:
+                st.Upload(buffer)
+                out = st.Download(np.empty_like(buffer))
+            results.append((buffer.copy(), out))
+        (a, a_round), (b, b_round) = results
+        assert np.array_equal(a, b) and np.array_equal(a_round, a) and np.array_equal(b_round, b)
+        if n == 21:
+            want, _ = orc.noise_apply(3, 0.37, n - 1, orc.execute(circuit, psi), [0.5])
+            assert np.max(np.abs(b - want)) <= 1e-12
+    finally:
+        pinned.free()
+
+
 # ---------------------------------------------------------------- full-size properties
 
 def test_30_qubit_brick_round_trip_and_norm(gpu_context):
