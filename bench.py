@@ -46,6 +46,17 @@ def measured_peaks() -> tuple[dict, str]:
     return {"hbm_gbs": FALLBACK_HBM_GBS, "bf16_tflops": 1590.0}, "fallback"
 
 
+def fp64_roofline(flops_per_step: float, steps: int, seconds: float, launches: int, clocks: dict) -> dict:
+    """FP64 side of the pass roofline: the flops the compiled passes issue per launch, their rate,
+    and the CUDA-core FP64 peak (64 FMA = 128 flops per clock per SM, 148 SMs) at the median SM
+    clock sampled during the timed region (1965 MHz when no sample was taken)."""
+    mhz = clocks.get("sm_mhz") or 1965.0
+    peak = 128 * 148 * mhz * 1e6 / 1e12
+    achieved = flops_per_step * steps / seconds / 1e12
+    return {"achieved_tflops": achieved, "peak_tflops": peak, "frac": achieved / peak,
+            "flops_per_launch": flops_per_step / max(1, launches), "peak_source": "nominal at the sampled SM clock"}
+
+
 def profile_traffic(kernel_key: str) -> float | None:
     """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
     for f in sorted((ROOT / "profiles").glob("*.md")):
@@ -579,6 +590,10 @@ def main() -> None:
     # amplitude for a general unitary (a scaled rotation between deferred phases), 4 for a real one.
     dense = sum(1 for op in circuit.Operations if int(op.Kind) in (0, 6, 7, 15))
     flops = dense * amps * 8 * 2
+    # what the compiled passes issue: 8 flops per amplitude for a general 2x2 (Rx, U), 4 for a real
+    # one (H, Ry), against the FP64 peak of 64 FMA per clock per SM at the sampled SM clock
+    fp64_flops = amps * sum(8 if int(op.Kind) in (6, 15) else 4
+                            for op in circuit.Operations if int(op.Kind) in (0, 6, 7, 15))
     e2e = None
     if not args.no_e2e and precision == FP64:
         backend = B200StateVectorBackend(context=ctx)
@@ -597,6 +612,7 @@ def main() -> None:
         host.free()
         backend.Dispose()
 
+    fp64 = fp64_roofline(fp64_flops, args.steps, total, launches, clocks.summary())
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         state.Dispose()
@@ -619,7 +635,8 @@ def main() -> None:
                          "frac": achieved_gbs / hbm_peak, "traffic": traffic, "peak_source": peak_kind,
                          "kernel": kernel_key, "algorithmic_bytes_per_launch": bytes_per_launch,
                          "launch_ms": 1e3 * per_launch_s,
-                         "dense_2x2_equivalent_tflops": flops * args.steps / total / 1e12},
+                         "dense_2x2_equivalent_tflops": flops * args.steps / total / 1e12,
+                         "fp64": fp64, "bound_frac": max(achieved_gbs / hbm_peak, fp64["frac"])},
             "gpu_launches": args.steps * launches,
             "clocks": clocks.summary(),
             "wall_s_timed": wall,

@@ -28,7 +28,7 @@
 extern "C" {
 #endif
 
-#define QM_ABI_VERSION 1
+#define QM_ABI_VERSION 2  /* 2: qm_fused_pass_info gained qubits_out and out_bit (relabeling passes) */
 
 /* Status codes.  The right-hand comment is the exception the reference raises for
  * the same condition, which is what a .NET shim maps the code to. */
@@ -217,7 +217,10 @@ typedef struct qm_fused_pass_info {
     int32_t stages;          /* register layouts used by the pass */
     int8_t reg_in[4];        /* local register bits of the load layout */
     int8_t reg_out[4];       /* local register bits of the store layout */
-} qm_fused_pass_info;        /* 84 bytes */
+    int8_t qubits_out[16];   /* index bit each local bit is written to (a permutation of qubits[]
+                                when the pass relabels qubits, qubits[] otherwise) */
+    int8_t out_bit[16];      /* index bit written by each thread rank of the store layout */
+} qm_fused_pass_info;        /* 116 bytes */
 
 typedef struct qm_fused_op_info {
     uint8_t code;

@@ -56,7 +56,8 @@ class PauliTermC(C.Structure):
 class FusedPassInfo(C.Structure):
     _fields_ = [("block_qubits", C.c_int32), ("op_begin", C.c_int32), ("op_count", C.c_int32),
                 ("qubits", C.c_int32 * 14), ("block_mask", C.c_uint32), ("stages", C.c_int32),
-                ("reg_in", C.c_int8 * 4), ("reg_out", C.c_int8 * 4)]
+                ("reg_in", C.c_int8 * 4), ("reg_out", C.c_int8 * 4), ("qubits_out", C.c_int8 * 16),
+                ("out_bit", C.c_int8 * 16)]
 
 
 class FusedOpInfo(C.Structure):

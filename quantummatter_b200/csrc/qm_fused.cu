@@ -64,6 +64,19 @@ struct Layout {
     }
 };
 
+// Local index of thread t in a stage layout with lanes (OP_STAGE `reserved`): thread ranks 0..n-1
+// on the lanes, the others on the remaining non-register local bits in ascending order.
+__device__ __forceinline__ uint32_t lane_base(uint32_t t, uint32_t regs, uint32_t code, int K) {
+    const int n = (int)(code & 15u);
+    uint32_t base = 0, used = regs;
+    for (int r = 0; r < n; ++r) {
+        const uint32_t b = (code >> (4 + 4 * r)) & 15u;
+        base |= ((t >> r) & 1u) << b;
+        used |= 1u << b;
+    }
+    return base | deposit(t >> n, ((1u << K) - 1u) & ~used);
+}
+
 // Registers whose index has bit m set, as a 2^R-bit pattern.
 __host__ __device__ constexpr uint32_t reg_half(int m) {
     uint32_t p = 0;
@@ -508,7 +521,7 @@ __global__ void __launch_bounds__(1 << (K - R), ((sizeof(T) == 8 && K == 12) || 
                     L.pm[m] = 1u << op.reg_pos[m];
                     regs |= L.pm[m];
                 }
-                L.base = deposit(t, ((1u << K) - 1u) & ~regs);
+                L.base = op.reserved ? lane_base(t, regs, op.reserved, K) : deposit(t, ((1u << K) - 1u) & ~regs);
                 slots<T>(L, sl);
                 __syncthreads();
 #pragma unroll
@@ -565,8 +578,10 @@ __global__ void __launch_bounds__(1 << (K - R), ((sizeof(T) == 8 && K == 12) || 
             }
         }
 
-        // the planner ends every pass in the store layout
-        const uint32_t g0 = outer | deposit(t, P.thread_out);
+        // the planner ends every pass in the store layout; thread rank r writes index bit out_bit[r]
+        uint32_t g0 = outer;
+#pragma unroll
+        for (int r = 0; r < K - R; ++r) g0 |= ((t >> r) & 1u) << P.out_bit[r];
 #pragma unroll
         for (int i = 0; i < NR; ++i) {
             uint32_t g = g0;
@@ -624,7 +639,7 @@ FusedLaunch fused_launch_params(int qubits, const FusedPass& p, const FusedOp* d
     for (int m = 0; m < R; ++m) {
         L.reg_in_l[m] = p.reg_in[m];
         L.reg_in_g[m] = 1u << p.q[p.reg_in[m]];
-        L.reg_out_g[m] = 1u << p.q[p.reg_out[m]];
+        L.reg_out_g[m] = 1u << p.q_out[p.reg_out[m]];
         reg_in_local |= 1u << p.reg_in[m];
         reg_out_local |= 1u << p.reg_out[m];
     }
@@ -632,8 +647,9 @@ FusedLaunch fused_launch_params(int qubits, const FusedPass& p, const FusedOp* d
     L.thread_out = 0;
     for (int b = 0; b < K; ++b) {
         if (!(reg_in_local & (1u << b))) L.thread_in |= 1u << p.q[b];
-        if (!(reg_out_local & (1u << b))) L.thread_out |= 1u << p.q[b];
+        if (!(reg_out_local & (1u << b))) L.thread_out |= 1u << p.q_out[b];
     }
+    for (int r = 0; r < 16; ++r) L.out_bit[r] = r < K - R ? (uint8_t)p.out_bit[r] : 0;
     L.op_count = p.op_count;
     L.ops = d_ops + p.op_begin;
     L.cta_shift = qubits - K;

@@ -65,7 +65,8 @@ constexpr uint16_t kOpBranch = 8;   // FusedOp::flags: a table op realising a no
 constexpr int32_t kSlotBranch = 1 << 24;
 
 enum OpCode : uint8_t {
-    OP_STAGE = 0,       // new register layout: reg_pos[0..R) local bit positions
+    OP_STAGE = 0,       // new register layout: reg_pos[0..R) local bit positions; `reserved` may name
+                        // the local bits of the lowest thread ranks (stage_lanes)
     OP_MATRIX = 1,      // complex 2x2 on register bit `reg`
     OP_MATRIX_REAL = 2, // real 2x2 (imaginary parts all zero)
     OP_EXCHANGE = 3,    // X on register bit `reg`
@@ -90,7 +91,7 @@ struct FusedOp {            // 88 bytes
     double coef[8];         // a, b, c, d as (re, im)
 };
 
-struct FusedPass {                  // 84 bytes
+struct FusedPass {                  // 116 bytes
     int32_t k;                      // block qubits
     int32_t op_begin, op_count;     // range in the plan's op array
     int32_t q[kMaxBlockQubits];     // block qubits, ascending
@@ -98,7 +99,18 @@ struct FusedPass {                  // 84 bytes
     int32_t stages;                 // number of register layouts
     int8_t reg_in[4];               // local register bits of the load layout (ascending; kRegBits used)
     int8_t reg_out[4];              // local register bits of the store layout (ascending; kRegBits used)
+    // Local bit b is read from index bit q[b] and written to index bit q_out[b]: a permutation of
+    // the block's bits when the pass relabels qubits, q itself otherwise.  Thread rank r of the
+    // store layout writes index bit out_bit[r].
+    int8_t q_out[16];
+    int8_t out_bit[16];
 };
+
+// OP_STAGE lane order: `reserved` = n | lane[0] << 4 | lane[1] << 8 | ...; thread ranks 0..n-1 take
+// local bits lane[0..n-1], the other thread ranks the remaining non-register local bits in
+// ascending order.  n = 0: all thread ranks in ascending order.
+inline int stage_lane_count(uint32_t reserved) { return (int)(reserved & 15u); }
+inline int stage_lane(uint32_t reserved, int i) { return (int)((reserved >> (4 + 4 * i)) & 15u); }
 
 struct Plan {
     int32_t qubits = 0;
@@ -177,6 +189,7 @@ struct FusedLaunch {
     const double* table;
     uint64_t state_stride;
     uint64_t table_stride;
+    uint8_t out_bit[16];        // index bit written by each thread rank at store (FusedPass::out_bit)
 };
 FusedLaunch fused_launch_params(int qubits, const FusedPass& p, const FusedOp* d_ops, const FusedBatch* batch);
 

@@ -11,7 +11,9 @@
 //   - the control predicates: register bits select pairs at compile time, thread bits become
 //     one uniform test per op, bits outside the block one test per work item;
 //   - an X, CNOT or SWAP acting on register bits only renames registers: no instruction;
-//   - the load, store and shared-memory exchange addresses as constants and bit deposits;
+//   - the load, store and shared-memory exchange addresses as constants and bit deposits,
+//     including a relabeling pass's store (qubits written to other index bits of the block)
+//     and the lane order a stage may set for it;
 //   - uncontrolled 2x2 unitaries as scaled rotations between deferred phases (below), with the
 //     phases carried from pass to pass of a plan;
 //   - from 26 qubits, the copy of the next work item's tile during the current one;
@@ -44,7 +46,8 @@ namespace qm {
 namespace {
 
 static_assert(sizeof(FusedOp) == 88, "FusedOp layout is mirrored in the generated source");
-static_assert(sizeof(FusedLaunch) == 112, "FusedLaunch layout is mirrored in the generated source");
+static_assert(sizeof(FusedLaunch) == 128 && offsetof(FusedLaunch, out_bit) == 112,
+              "FusedLaunch layout is mirrored in the generated source");
 static_assert(offsetof(FusedLaunch, ops) == 80 && offsetof(FusedLaunch, table) == 88 &&
                   offsetof(FusedLaunch, state_stride) == 96 && offsetof(FusedLaunch, table_stride) == 104,
               "FusedLaunch layout is mirrored in the generated source");
@@ -119,6 +122,21 @@ std::string deposit_expr(const char* value, uint32_t mask) {
         e << " | (((" << value << " >> " << src << ") & " << hexu(ones) << ") << " << b << ")";
         src += len;
         b += len;
+    }
+    e << ")";
+    return e.str();
+}
+
+// bit r of value moved to bit bits[r] (r < n), as shifts of runs
+std::string permute_expr(const char* value, const int8_t* bits, int n) {
+    std::ostringstream e;
+    e << "(0u";
+    for (int r = 0; r < n;) {
+        int len = 1;
+        while (r + len < n && bits[r + len] == bits[r] + len) ++len;
+        const uint32_t ones = (1u << len) - 1u;
+        e << " | (((" << value << " >> " << r << ") & " << hexu(ones) << ") << " << (int)bits[r] << ")";
+        r += len;
     }
     e << ")";
     return e.str();
@@ -233,6 +251,7 @@ struct FusedLaunch {
     const FusedOp* ops;
     const double* table;
     u64 state_stride, table_stride;
+    unsigned char out_bit[16];
 };
 __device__ __forceinline__ u32 qm_deposit(u32 value, u32 mask) {
     u32 out = 0;
@@ -258,6 +277,7 @@ struct Gen {
     std::vector<Pend> pend;
     cplx G{1.0, 0.0};
     int uid = 0;
+    uint32_t lanes = 0;  // lane order of the current layout (OP_STAGE `reserved`; 0: ascending)
 
     std::string X(int i) const { return "x" + std::to_string(phys[i]); }
     std::string Y(int i) const { return "y" + std::to_string(phys[i]); }
@@ -288,7 +308,20 @@ struct Gen {
     void set_layout(const int8_t* pos) {
         for (int m = 0; m < R; ++m) pm[m] = 1u << pos[m];
     }
-    std::string base_expr() const { return deposit_expr("t", ((1u << K) - 1u) & ~regmask()); }
+    // thread t's local index: thread ranks on the lanes first (when the layout has lanes), then
+    // on the remaining non-register local bits in ascending order
+    std::string base_expr() const {
+        uint32_t free = ((1u << K) - 1u) & ~regmask();
+        const int n = stage_lane_count(lanes);
+        if (n == 0) return deposit_expr("t", free);
+        int8_t lb[8];
+        for (int r = 0; r < n; ++r) {
+            lb[r] = (int8_t)stage_lane(lanes, r);
+            free &= ~(1u << lb[r]);
+        }
+        const std::string rest = "(t >> " + std::to_string(n) + ")";
+        return "(" + permute_expr("t", lb, n) + " | " + deposit_expr(rest.c_str(), free) + ")";
+    }
 
     // opens runtime conditions for outer and thread control bits; returns how many to close
     int open_conditions(uint32_t outer_bits, uint32_t thread_bits) {
@@ -353,12 +386,13 @@ struct Gen {
                << Y(pr.second) << " = u; }\n";
     }
 
-    void stage(const int8_t* pos) {
+    void stage(const int8_t* pos, uint32_t lane_code) {
         os << "{ const u32 sb = qm_swz(base);\n__syncthreads();\n";
         for (int i = 0; i < NR; ++i) {
             os << "{ V v; v.x = " << X(i) << "; v.y = " << Y(i) << "; tile[sb ^ " << hexu(const_slot(i)) << "] = v; }\n";
         }
         set_layout(pos);
+        lanes = lane_code;
         for (int i = 0; i < NR; ++i) phys[i] = i;
         os << "base = " << base_expr() << ";\n";
         os << "const u32 sn = qm_swz(base);\n__syncthreads();\n";
@@ -864,17 +898,15 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int
         g.G = carry->g;
         g.normalize();
     }
-    uint32_t thread_in = 0, thread_out = 0, reg_in_local = 0, reg_out_local = 0;
+    uint32_t thread_in = 0, reg_in_local = 0;
     uint32_t reg_in_g[R], reg_out_g[R];
     for (int m = 0; m < R; ++m) {
         reg_in_local |= 1u << p.reg_in[m];
-        reg_out_local |= 1u << p.reg_out[m];
         reg_in_g[m] = 1u << p.q[p.reg_in[m]];
-        reg_out_g[m] = 1u << p.q[p.reg_out[m]];
+        reg_out_g[m] = 1u << p.q_out[p.reg_out[m]];
     }
     for (int b = 0; b < p.k; ++b) {
         if (!(reg_in_local & (1u << b))) thread_in |= 1u << p.q[b];
-        if (!(reg_out_local & (1u << b))) thread_out |= 1u << p.q[b];
     }
     const int nt = 1 << (p.k - R);
     const size_t tile_bytes = (size_t)(fp64 ? 16 : 8) << p.k;
@@ -892,7 +924,15 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int
     // partial row u = state * rows + r always holds the same tiles [r C, (r + 1) C) of its state
     // (rows = 2^(n-16), the layout of launch_group_histogram), whatever the state's place in the
     // batch.  Within a chunk the bins accumulate per warp in shared memory in a fixed order.
-    const bool hist = hist_mask != 0 && __builtin_popcount(hist_mask) <= kGroupMaxBits;
+    // a relabeling pass (qubits written to other bits, lanes in a stage) keeps the separate
+    // joint-mass kernel: the epilogue reads the bins in the unpermuted, ascending layout
+    bool relabels = false;
+    for (int b = 0; b < p.k; ++b) relabels |= p.q_out[b] != p.q[b];
+    for (int o = 0; o < p.op_count; ++o) {
+        const FusedOp& op = plan_ops[(size_t)(p.op_begin + o)];
+        relabels |= op.code == OP_STAGE && op.reserved != 0;
+    }
+    const bool hist = hist_mask != 0 && __builtin_popcount(hist_mask) <= kGroupMaxBits && !relabels;
     const int hist_bins = hist ? 1 << __builtin_popcount(hist_mask) : 0;
     const int chunk = hist ? (qubits > 16 ? 1 << (16 - p.k) : 1 << (qubits - p.k)) : 1;
     const int warps = nt / 32;
@@ -1001,7 +1041,7 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int
     for (int o = 0; o < p.op_count; ++o) {
         const FusedOp& op = plan_ops[(size_t)(p.op_begin + o)];
         if (op.code == OP_STAGE) {
-            g.stage(op.reg_pos);
+            g.stage(op.reg_pos, op.reserved);
             if (late && o == last_stage) {
                 os << "__syncthreads();\n";  // every thread has read the exchange tile
                 prefetch("item + gridDim.x");
@@ -1025,8 +1065,8 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int
         carry->pend.clear();
         for (const Pend& e : g.pend) {
             uint32_t gm = e.omask;
-            for (int b = 0; b < p.k; ++b)
-                if (e.lmask & (1u << b)) gm |= 1u << p.q[b];
+            for (int b = 0; b < p.k; ++b)  // where the pass writes each local bit
+                if (e.lmask & (1u << b)) gm |= 1u << p.q_out[b];
             carry->pend.push_back({gm, e.v});
         }
         carry->g = g.G;
@@ -1084,7 +1124,7 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int
         }
         os << "}\n";
     }
-    os << "{ const u32 g1 = outer | " << deposit_expr("t", thread_out) << ";\n";
+    os << "{ const u32 g1 = outer | " << permute_expr("t", p.out_bit, p.k - R) << ";\n";
     for (int i = 0; i < NR; ++i) {
         uint32_t gi = 0;
         for (int m = 0; m < R; ++m)

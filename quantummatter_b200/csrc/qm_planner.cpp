@@ -14,6 +14,7 @@
 // Diagonal gates never need block or register space: their phase is a function of the
 // global index, which every amplitude knows.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -58,6 +59,20 @@ GInfo classify(const qm_gate& g) {
 }
 
 inline bool blocked(const GInfo& g, uint32_t bx, uint32_t bz) { return (g.touch & bx) || (g.xmask & bz); }
+
+// a gate's qubits renamed by a permutation of the index bits
+void remap_gate(GInfo& gi, const int* perm) {
+    qm_gate g = gi.g;
+    g.target = perm[g.target];
+    uint32_t cm = 0;
+    for (int q = 0; q < 32; ++q)
+        if (g.control_mask & (1u << q)) cm |= 1u << perm[q];
+    g.control_mask = cm;
+    if (g.kernel == QM_KERNEL_SWAP) g.swap_control = perm[g.swap_control];
+    const int32_t slot = gi.slot;
+    gi = classify(g);
+    gi.slot = slot;
+}
 
 inline bool is_exact(const double* v, double re, double im) { return v[0] == re && v[1] == im; }
 
@@ -155,6 +170,397 @@ bool plan_fused(const std::vector<qm_gate>& gates, int qubits, int precision, in
     const int low_bits = precision == QM_FP32 ? 4 : 3;
     const uint32_t low_mask = (1u << low_bits) - 1u;
 
+    // Relabeling (plans without per-state coefficients): a pass may write its tile back with the
+    // block's qubits permuted among the block's index bits.  Index bits 0..low_bits-1 (the run
+    // every pass reads whole) then hold the qubits the next pass can use best, found by trying
+    // every choice against the next pass's greedy absorption, and the remaining gates are
+    // renamed to match.  Blocks then follow the circuit's light cone instead of carrying qubits
+    // 0..low_bits-1 through every pass.  `at[b]` is the qubit held at index bit b; the last
+    // passes put every qubit back at its own bit.
+    static const bool relabel_env = [] {
+        const char* e = std::getenv("QM_RELABEL");
+        return !(e && e[0] == '0');
+    }();
+    const bool relabel = relabel_env && !slots && qubits > k;
+    const uint32_t all_qubits = qubits >= 32 ? 0xffffffffu : (1u << qubits) - 1u;
+    int at[32];
+    for (int q = 0; q < 32; ++q) at[q] = q;
+    int perm[32];
+    int lane_pos[8];
+
+    auto build_pass = [&](uint32_t Q, const std::vector<GInfo>& absorbed) -> bool {
+            FusedPass pass{};
+            pass.k = k;
+            pass.block_mask = Q;
+            int local_of[32];
+            for (int i = 0; i < 32; ++i) local_of[i] = -1;
+            int nb = 0;
+            for (int q = 0; q < qubits; ++q)
+                if (Q & (1u << q)) {
+                    local_of[q] = nb;
+                    pass.q[nb++] = q;
+                }
+            for (int b = 0; b < 16; ++b) pass.q_out[b] = pass.out_bit[b] = -1;
+            for (int b = 0; b < k; ++b) pass.q_out[b] = (int8_t)perm[pass.q[b]];
+            // lanes: the local bits whose qubits go to index bits 0..low_bits-1, in that order; they
+            // must be the lowest thread ranks of the store layout (the coalesced run)
+            uint32_t lane_mask = 0, lane_code = 0;
+            bool lanes_needed = false;
+            for (int r = 0; r < low_bits; ++r) {
+                const int lb = local_of[lane_pos[r]];
+                lane_mask |= 1u << lb;
+                lane_code |= (uint32_t)lb << (4 + 4 * r);
+                if (lb != r) lanes_needed = true;
+            }
+            lane_code |= (uint32_t)low_bits;
+            pass.op_begin = (int32_t)plan.ops.size();
+            auto to_local = [&](uint32_t global) {
+                uint32_t l = 0;
+                for (int q = 0; q < qubits; ++q)
+                    if (global & (1u << q)) l |= 1u << local_of[q];
+                return l;
+            };
+
+            // 1) split the pass into stages: each stage holds gates whose register needs fit in
+            //    kRegBits qubits, in commutation-respecting order
+            std::vector<std::vector<GInfo>> stage_gates;
+            std::vector<uint32_t> stage_need;  // local bits
+            std::vector<uint32_t> stage_soft;  // local bits worth holding (controls of X gates)
+            {
+                std::vector<GInfo> pending = absorbed;
+                while (!pending.empty()) {
+                    uint32_t P = 0, sbx = 0, sbz = 0;
+                    std::vector<GInfo> mine, later;
+                    for (const GInfo& g : pending) {
+                        if (!blocked(g, sbx, sbz)) {
+                            if (g.diag) {
+                                mine.push_back(g);
+                                continue;
+                            }
+                            uint32_t np = P | g.need;
+                            if (popc(np) <= kRegBits) {
+                                P = np;
+                                mine.push_back(g);
+                                continue;
+                            }
+                        }
+                        later.push_back(g);
+                        sbx |= g.xmask;
+                        sbz |= g.zmask;
+                    }
+                    // controls of X gates are worth holding in registers too: the X then becomes
+                    // a fixed register permutation
+                    uint32_t soft = 0;
+                    for (const GInfo& g : mine)
+                        if (g.g.kernel == QM_KERNEL_EXCHANGE) soft |= g.g.control_mask & Q;
+                    stage_gates.push_back(mine);
+                    stage_need.push_back(to_local(P));
+                    stage_soft.push_back(to_local(soft) & ~((1u << low_bits) - 1u));
+                    pending.swap(later);
+                }
+            }
+            // 2) register layouts: keep the current layout when it already covers a stage's
+            //    needs; otherwise take the needs, then the next stages' needs (so the following
+            //    stage may not need a change), then the current layout, then the highest bits.
+            //    Low local bits (the coalescing run) are never used as filler.
+            const uint32_t low_local = (1u << low_bits) - 1u;
+            const uint32_t canonical = ((1u << kRegBits) - 1u) << (k - kRegBits);
+            auto fill = [&](uint32_t need, size_t from, uint32_t current) {
+                uint32_t l = need;
+                if (from >= 1 && from - 1 < stage_soft.size()) {
+                    uint32_t soft = stage_soft[from - 1] & ~l;
+                    for (int b = 0; b < k && popc(l) < kRegBits; ++b)
+                        if (soft & (1u << b)) l |= 1u << b;
+                }
+                for (size_t s = from; s < stage_need.size() && popc(l) < kRegBits; ++s) {
+                    uint32_t extra = stage_need[s] & ~l & ~low_local;
+                    for (int b = 0; b < k && popc(l) < kRegBits; ++b)
+                        if (extra & (1u << b)) l |= 1u << b;
+                }
+                // relabeling passes keep their lanes off the filler, so that the last layout can
+                // take the lane order without one more exchange
+                const uint32_t avoid = low_local | (lanes_needed ? lane_mask : 0u);
+                for (int b = k - 1; b >= 0 && popc(l) < kRegBits; --b)
+                    if ((current & (1u << b)) && !(avoid & (1u << b))) l |= 1u << b;
+                for (int b = k - 1; b >= 0 && popc(l) < kRegBits; --b)
+                    if (!(avoid & (1u << b))) l |= 1u << b;
+                for (int b = k - 1; b >= 0 && popc(l) < kRegBits; --b)
+                    if (!(low_local & (1u << b))) l |= 1u << b;
+                return l;
+            };
+            auto emit_stage = [&](uint32_t layout) {
+                FusedOp st{};
+                st.code = OP_STAGE;
+                st.reg = st.reg2 = st.local = -1;
+                int m = 0;
+                for (int b = 0; b < k; ++b)
+                    if (layout & (1u << b)) st.reg_pos[m++] = (int8_t)b;
+                plan.ops.push_back(st);
+            };
+            auto set_regs = [&](int8_t* dst, uint32_t layout) {
+                int m = 0;
+                for (int b = 0; b < k; ++b)
+                    if (layout & (1u << b)) dst[m++] = (int8_t)b;
+            };
+            uint32_t layout = fill(stage_need.empty() ? 0 : stage_need[0], 1, canonical);
+            int stages = 1;
+            if (layout & low_local) {
+                set_regs(pass.reg_in, canonical);
+                emit_stage(layout);
+                ++stages;
+            } else {
+                set_regs(pass.reg_in, layout);
+            }
+            for (size_t si = 0; si < stage_gates.size(); ++si) {
+                if ((stage_need[si] & ~layout) != 0) {
+                    layout = fill(stage_need[si], si + 1, layout);
+                    emit_stage(layout);
+                    ++stages;
+                }
+                int reg_of_local[32];
+                for (int i = 0; i < 32; ++i) reg_of_local[i] = -1;
+                {
+                    int m = 0;
+                    for (int b = 0; b < k; ++b)
+                        if (layout & (1u << b)) reg_of_local[b] = m++;
+                }
+                // Commuting diagonals (uncontrolled phases, CZ/Z negates) collect in a group that is
+                // emitted as one OP_DIAG_GROUP; a non-diagonal gate may run ahead of the group when
+                // its target is none of the group's qubits (they commute), otherwise the group is
+                // emitted first.
+                std::vector<FusedOp> group;
+                uint32_t group_qubits = 0;
+                auto flush = [&]() {
+                    if (group.size() > 1) {
+                        FusedOp hdr{};
+                        hdr.code = OP_DIAG_GROUP;
+                        hdr.reg = hdr.reg2 = hdr.local = -1;
+                        hdr.reserved = (uint32_t)group.size();
+                        plan.ops.push_back(hdr);
+                    }
+                    for (const FusedOp& m : group) plan.ops.push_back(m);
+                    group.clear();
+                    group_qubits = 0;
+                };
+                for (const GInfo& gi : stage_gates[si]) {
+                    const qm_gate& g = gi.g;
+                    FusedOp op{};
+                    op.reg = op.reg2 = -1;
+                    op.local = -1;
+                    for (int q = 0; q < qubits; ++q) {
+                        if (!(g.control_mask & (1u << q))) continue;
+                        if (local_of[q] >= 0) op.cmask_local |= (uint16_t)(1u << local_of[q]);
+                        else op.cmask_outer |= 1u << q;
+                    }
+                    std::memcpy(&op.coef[0], g.a, 16);
+                    std::memcpy(&op.coef[2], g.b, 16);
+                    std::memcpy(&op.coef[4], g.c, 16);
+                    std::memcpy(&op.coef[6], g.d, 16);
+                    if (gi.slot >= 0 && (gi.slot & kSlotBranch)) {
+                        // noise branch: per-state coefficients, tested at run time
+                        op.flags = kOpTable | kOpBranch;
+                        op.reserved = (uint32_t)(gi.slot & (kSlotBranch - 1));
+                        op.code = OP_MATRIX;
+                        op.reg = (int8_t)reg_of_local[local_of[g.target]];
+                    } else if (gi.slot >= 0) {
+                        // per-state coefficients: generic op reading the batch table
+                        op.flags = kOpTable;
+                        op.reserved = (uint32_t)gi.slot;
+                        if (gi.diag) {
+                            int lt = local_of[g.target];
+                            op.code = OP_DIAG;
+                            op.local = (int8_t)lt;
+                            op.target_outer = lt >= 0 ? 0u : (1u << g.target);
+                        } else {
+                            bool real = g.a[1] == 0 && g.b[1] == 0 && g.c[1] == 0 && g.d[1] == 0;
+                            op.code = real ? OP_MATRIX_REAL : OP_MATRIX;
+                            op.reg = (int8_t)reg_of_local[local_of[g.target]];
+                        }
+                    } else if (gi.diag) {
+                        bool a1 = is_exact(g.a, 1.0, 0.0), d1 = is_exact(g.d, 1.0, 0.0);
+                        int lt = local_of[g.target];
+                        if (a1 && is_exact(g.d, -1.0, 0.0)) {
+                            op.code = OP_NEGATE;
+                            if (lt >= 0) op.cmask_local |= (uint16_t)(1u << lt);
+                            else op.cmask_outer |= 1u << g.target;
+                        } else {
+                            op.code = OP_DIAG;
+                            op.local = (int8_t)lt;
+                            op.target_outer = lt >= 0 ? 0u : (1u << g.target);
+                            op.flags = (uint16_t)((a1 ? 1 : 0) | (d1 ? 2 : 0));
+                        }
+                    } else if (g.kernel == QM_KERNEL_EXCHANGE) {
+                        op.code = OP_EXCHANGE;
+                        op.reg = (int8_t)reg_of_local[local_of[g.target]];
+                        for (int q = 0; q < qubits && op.reg2 < 0; ++q)
+                            if ((g.control_mask & (1u << q)) && local_of[q] >= 0 && reg_of_local[local_of[q]] >= 0)
+                                op.reg2 = (int8_t)reg_of_local[local_of[q]];
+                    } else if (g.kernel == QM_KERNEL_SWAP) {
+                        op.code = OP_SWAP;
+                        op.reg = (int8_t)reg_of_local[local_of[g.target]];
+                        op.reg2 = (int8_t)reg_of_local[local_of[g.swap_control]];
+                    } else {
+                        bool real = g.a[1] == 0 && g.b[1] == 0 && g.c[1] == 0 && g.d[1] == 0;
+                        op.code = real ? OP_MATRIX_REAL : OP_MATRIX;
+                        op.reg = (int8_t)reg_of_local[local_of[g.target]];
+                    }
+                    if ((op.code == OP_MATRIX || op.code == OP_MATRIX_REAL || op.code == OP_EXCHANGE) && op.reg < 0) {
+                        error = "planner placed a gate outside the register layout";
+                        return false;
+                    }
+                    if (op.code == OP_SWAP && (op.reg < 0 || op.reg2 < 0)) {
+                        error = "planner placed a swap outside the register layout";
+                        return false;
+                    }
+                    const bool groupable =
+                        (op.code == OP_DIAG && op.cmask_local == 0 && op.cmask_outer == 0) ||
+                        (op.code == OP_NEGATE && popc(op.cmask_local) + popc(op.cmask_outer) <= 2);
+                    if (groupable) {
+                        group.push_back(op);
+                        group_qubits |= gi.touch;
+                        continue;
+                    }
+                    if (!gi.diag && (gi.xmask & group_qubits)) flush();
+                    plan.ops.push_back(op);
+                }
+                flush();
+            }
+            if (lanes_needed) {
+                // the store layout keeps the lanes on thread bits, as the lowest thread ranks: the
+                // pass's last stage takes the lane order when its registers leave the lanes free,
+                // otherwise one more stage does
+                int last_stage = -1;
+                for (size_t o = (size_t)pass.op_begin; o < plan.ops.size(); ++o)
+                    if (plan.ops[o].code == OP_STAGE) last_stage = (int)o;
+                if (last_stage < 0 || (layout & lane_mask)) {
+                    uint32_t l = layout & ~lane_mask;
+                    for (int b = k - 1; b >= 0 && popc(l) < kRegBits; --b)
+                        if (!(lane_mask & (1u << b))) l |= 1u << b;
+                    layout = l;
+                    emit_stage(layout);
+                    ++stages;
+                    last_stage = (int)plan.ops.size() - 1;
+                }
+                plan.ops[(size_t)last_stage].reserved = lane_code;
+                set_regs(pass.reg_out, layout);
+            } else if (layout & low_local) {
+                emit_stage(canonical);
+                ++stages;
+                set_regs(pass.reg_out, canonical);
+                layout = canonical;
+            } else {
+                set_regs(pass.reg_out, layout);
+            }
+            {
+                // Without a stage nothing orders one thread's stores after another's loads: a
+                // relabeling pass stores through another mapping than it loads, so a thread could
+                // overwrite an amplitude of its tile before the thread that loads it has.  Such a
+                // pass (a restoring pass without gates) takes one exchange in its store layout,
+                // whose barriers order them.
+                bool moves = false, staged = false;
+                for (int b = 0; b < k; ++b) moves |= pass.q_out[b] != pass.q[b];
+                for (size_t o = (size_t)pass.op_begin; o < plan.ops.size(); ++o) staged |= plan.ops[o].code == OP_STAGE;
+                if (moves && !staged) {
+                    emit_stage(layout);
+                    ++stages;
+                }
+            }
+            {
+                // store order: the lanes (when given), then the other thread bits ascending
+                int rank = 0;
+                if (lanes_needed)
+                    for (int r = 0; r < low_bits; ++r) pass.out_bit[rank++] = pass.q_out[stage_lane(lane_code, r)];
+                for (int b = 0; b < k; ++b)
+                    if (!(layout & (1u << b)) && !(lanes_needed && (lane_mask & (1u << b))))
+                        pass.out_bit[rank++] = pass.q_out[b];
+                for (int r = 0; r < low_bits; ++r)
+                    if (pass.out_bit[r] != r) {
+                        error = "planner lost the coalesced run of a store layout";
+                        return false;
+                    }
+            }
+            pass.op_count = (int32_t)plan.ops.size() - pass.op_begin;
+            if (pass.op_count > kMaxPassOps) {
+                error = "pass program exceeds the kernel-parameter capacity";
+                return false;
+            }
+            pass.stages = stages;
+            plan.passes.push_back(pass);
+            plan.planned_bytes += 2 * n * elem;
+            return true;
+    };
+
+    // where each qubit of block Q goes: the qubits at lane_pos[r] to index bit r, every other
+    // qubit to its own bit when that bit is a free one of the block, else where it is when that is
+    // free, else to the lowest free bit
+    auto place = [&](uint32_t Q) {
+        for (int q = 0; q < 32; ++q) perm[q] = q;
+        uint32_t lanes = 0;
+        for (int r = 0; r < low_bits; ++r) {
+            perm[lane_pos[r]] = r;
+            lanes |= 1u << lane_pos[r];
+        }
+        uint32_t open = Q & ~low_mask, todo = Q & ~lanes;
+        for (int b = 0; b < 32; ++b)
+            if ((todo >> b) & 1u) {
+                const int home = at[b];
+                if (home >= low_bits && ((open >> home) & 1u)) {
+                    perm[b] = home;
+                    open &= ~(1u << home);
+                    todo &= ~(1u << b);
+                }
+            }
+        for (int b = 0; b < 32; ++b)
+            if (((todo >> b) & 1u) && ((open >> b) & 1u)) {
+                open &= ~(1u << b);
+                todo &= ~(1u << b);
+            }
+        for (int b = 0; b < 32; ++b)
+            if ((todo >> b) & 1u) {
+                const int to = __builtin_ctz(open);
+                perm[b] = to;
+                open &= ~(1u << to);
+            }
+    };
+    // lanes from a set of low_bits index bits: a qubit 0..low_bits-1 to its own lane, the others
+    // in ascending order
+    auto set_lanes = [&](uint32_t F) {
+        bool used[8] = {};
+        for (int r = 0; r < low_bits; ++r) lane_pos[r] = -1;
+        for (int b = 0; b < 32; ++b)
+            if (((F >> b) & 1u) && at[b] < low_bits && !used[at[b]]) {
+                lane_pos[at[b]] = b;
+                used[at[b]] = true;
+                F &= ~(1u << b);
+            }
+        for (int r = 0; r < low_bits; ++r)
+            if (lane_pos[r] < 0) {
+                lane_pos[r] = __builtin_ctz(F);
+                F &= ~(1u << lane_pos[r]);
+            }
+    };
+    auto apply = [&](std::vector<GInfo>& gates) {
+        int moved[32];
+        for (int q = 0; q < 32; ++q) moved[perm[q]] = at[q];
+        for (int q = 0; q < 32; ++q) at[q] = moved[q];
+        for (GInfo& g : gates) remap_gate(g, perm);
+    };
+    auto in_order = [&]() {
+        for (int q = 0; q < qubits; ++q)
+            if (at[q] != q) return false;
+        return true;
+    };
+    // index bits of qubits 0..low_bits-1, then of displaced qubits along their cycles, up to k
+    auto restoring_block = [&](uint32_t Q) {
+        for (int b = 0; b < qubits && popc(Q) < k; ++b)
+            if (at[b] < low_bits) Q |= 1u << b;
+        for (int b = 0; b < qubits && popc(Q) < k; ++b) {
+            if (at[b] == b || ((Q >> b) & 1u)) continue;
+            for (int c = b; popc(Q) < k && !((Q >> c) & 1u); c = at[c]) Q |= 1u << c;
+        }
+        return Q;
+    };
+
     while (!remaining.empty()) {
         uint32_t Q = low_mask;
         uint32_t bx = 0, bz = 0;
@@ -182,242 +588,84 @@ bool plan_fused(const std::vector<qm_gate>& gates, int qubits, int precision, in
             uint32_t extra = g.need & ~Q;
             if (extra && popc(Q | extra) <= k) Q |= extra;
         }
+        // the last pass of the circuit takes the bits that put qubits back before the lowest ones
+        if (relabel && rest.empty()) Q = restoring_block(Q);
         for (int q = 0; q < qubits && popc(Q) < k; ++q) Q |= 1u << q;
 
-        FusedPass pass{};
-        pass.k = k;
-        pass.block_mask = Q;
-        int local_of[32];
-        for (int i = 0; i < 32; ++i) local_of[i] = -1;
-        int nb = 0;
-        for (int q = 0; q < qubits; ++q)
-            if (Q & (1u << q)) {
-                local_of[q] = nb;
-                pass.q[nb++] = q;
-            }
-        pass.op_begin = (int32_t)plan.ops.size();
-        auto to_local = [&](uint32_t global) {
-            uint32_t l = 0;
-            for (int q = 0; q < qubits; ++q)
-                if (global & (1u << q)) l |= 1u << local_of[q];
-            return l;
-        };
-
-        // 1) split the pass into stages: each stage holds gates whose register needs fit in
-        //    kRegBits qubits, in commutation-respecting order
-        std::vector<std::vector<GInfo>> stage_gates;
-        std::vector<uint32_t> stage_need;  // local bits
-        std::vector<uint32_t> stage_soft;  // local bits worth holding (controls of X gates)
-        {
-            std::vector<GInfo> pending = absorbed;
-            while (!pending.empty()) {
-                uint32_t P = 0, sbx = 0, sbz = 0;
-                std::vector<GInfo> mine, later;
-                for (const GInfo& g : pending) {
-                    if (!blocked(g, sbx, sbz)) {
-                        if (g.diag) {
-                            mine.push_back(g);
-                            continue;
-                        }
-                        uint32_t np = P | g.need;
-                        if (popc(np) <= kRegBits) {
-                            P = np;
-                            mine.push_back(g);
+        for (int q = 0; q < 32; ++q) perm[q] = q;
+        for (int r = 0; r < low_bits; ++r) lane_pos[r] = r;
+        if (relabel && rest.empty()) {
+            // the last pass of the circuit starts putting the qubits back
+            uint32_t F = 0;
+            for (int b = 0; b < qubits; ++b)
+                if (at[b] < low_bits) F |= 1u << b;
+            if ((F & ~Q) == 0) set_lanes(F);
+            place(Q);
+        } else if (relabel) {
+            // the low_bits bits of Q whose qubits let the next pass absorb the most gates
+            auto absorbable = [&](uint32_t start) {
+                uint32_t QQ = start, cx = 0, cz = 0;
+                int c = 0;
+                for (const GInfo& g : rest) {
+                    if (c >= kMaxPassGates || cx == all_qubits) break;
+                    if (!blocked(g, cx, cz)) {
+                        const uint32_t nq = QQ | g.need;
+                        if (popc(nq) <= k) {
+                            QQ = nq;
+                            ++c;
                             continue;
                         }
                     }
-                    later.push_back(g);
-                    sbx |= g.xmask;
-                    sbz |= g.zmask;
+                    cx |= g.xmask;
+                    cz |= g.zmask;
                 }
-                // controls of X gates are worth holding in registers too: the X then becomes
-                // a fixed register permutation
-                uint32_t soft = 0;
-                for (const GInfo& g : mine)
-                    if (g.g.kernel == QM_KERNEL_EXCHANGE) soft |= g.g.control_mask & Q;
-                stage_gates.push_back(mine);
-                stage_need.push_back(to_local(P));
-                stage_soft.push_back(to_local(soft) & ~((1u << low_bits) - 1u));
-                pending.swap(later);
-            }
-        }
-        // 2) register layouts: keep the current layout when it already covers a stage's
-        //    needs; otherwise take the needs, then the next stages' needs (so the following
-        //    stage may not need a change), then the current layout, then the highest bits.
-        //    Low local bits (the coalescing run) are never used as filler.
-        const uint32_t low_local = (1u << low_bits) - 1u;
-        const uint32_t canonical = ((1u << kRegBits) - 1u) << (k - kRegBits);
-        auto fill = [&](uint32_t need, size_t from, uint32_t current) {
-            uint32_t l = need;
-            if (from >= 1) {
-                uint32_t soft = stage_soft[from - 1] & ~l;
-                for (int b = 0; b < k && popc(l) < kRegBits; ++b)
-                    if (soft & (1u << b)) l |= 1u << b;
-            }
-            for (size_t s = from; s < stage_need.size() && popc(l) < kRegBits; ++s) {
-                uint32_t extra = stage_need[s] & ~l & ~low_local;
-                for (int b = 0; b < k && popc(l) < kRegBits; ++b)
-                    if (extra & (1u << b)) l |= 1u << b;
-            }
-            for (int b = k - 1; b >= 0 && popc(l) < kRegBits; --b)
-                if ((current & (1u << b)) && !(low_local & (1u << b))) l |= 1u << b;
-            for (int b = k - 1; b >= 0 && popc(l) < kRegBits; --b)
-                if (!(low_local & (1u << b))) l |= 1u << b;
-            return l;
-        };
-        auto emit_stage = [&](uint32_t layout) {
-            FusedOp st{};
-            st.code = OP_STAGE;
-            st.reg = st.reg2 = st.local = -1;
-            int m = 0;
-            for (int b = 0; b < k; ++b)
-                if (layout & (1u << b)) st.reg_pos[m++] = (int8_t)b;
-            plan.ops.push_back(st);
-        };
-        auto set_regs = [&](int8_t* dst, uint32_t layout) {
-            int m = 0;
-            for (int b = 0; b < k; ++b)
-                if (layout & (1u << b)) dst[m++] = (int8_t)b;
-        };
-        uint32_t layout = fill(stage_need.empty() ? 0 : stage_need[0], 1, canonical);
-        int stages = 1;
-        if (layout & low_local) {
-            set_regs(pass.reg_in, canonical);
-            emit_stage(layout);
-            ++stages;
-        } else {
-            set_regs(pass.reg_in, layout);
-        }
-        for (size_t si = 0; si < stage_gates.size(); ++si) {
-            if ((stage_need[si] & ~layout) != 0) {
-                layout = fill(stage_need[si], si + 1, layout);
-                emit_stage(layout);
-                ++stages;
-            }
-            int reg_of_local[32];
-            for (int i = 0; i < 32; ++i) reg_of_local[i] = -1;
-            {
-                int m = 0;
-                for (int b = 0; b < k; ++b)
-                    if (layout & (1u << b)) reg_of_local[b] = m++;
-            }
-            // Commuting diagonals (uncontrolled phases, CZ/Z negates) collect in a group that is
-            // emitted as one OP_DIAG_GROUP; a non-diagonal gate may run ahead of the group when
-            // its target is none of the group's qubits (they commute), otherwise the group is
-            // emitted first.
-            std::vector<FusedOp> group;
-            uint32_t group_qubits = 0;
-            auto flush = [&]() {
-                if (group.size() > 1) {
-                    FusedOp hdr{};
-                    hdr.code = OP_DIAG_GROUP;
-                    hdr.reg = hdr.reg2 = hdr.local = -1;
-                    hdr.reserved = (uint32_t)group.size();
-                    plan.ops.push_back(hdr);
-                }
-                for (const FusedOp& m : group) plan.ops.push_back(m);
-                group.clear();
-                group_qubits = 0;
+                return c;
             };
-            for (const GInfo& gi : stage_gates[si]) {
-                const qm_gate& g = gi.g;
-                FusedOp op{};
-                op.reg = op.reg2 = -1;
-                op.local = -1;
-                for (int q = 0; q < qubits; ++q) {
-                    if (!(g.control_mask & (1u << q))) continue;
-                    if (local_of[q] >= 0) op.cmask_local |= (uint16_t)(1u << local_of[q]);
-                    else op.cmask_outer |= 1u << q;
+            int bits[32], nb = 0;
+            for (int b = 0; b < qubits; ++b)
+                if ((Q >> b) & 1u) bits[nb++] = b;
+            int best = -1;
+            uint32_t bestF = low_mask;
+            int idx[8];
+            for (int i = 0; i < low_bits; ++i) idx[i] = i;
+            while (true) {
+                uint32_t F = 0;
+                for (int i = 0; i < low_bits; ++i) F |= 1u << bits[idx[i]];
+                const int score = 2 * absorbable(F) + (F == low_mask ? 1 : 0);
+                if (score > best) {
+                    best = score;
+                    bestF = F;
                 }
-                std::memcpy(&op.coef[0], g.a, 16);
-                std::memcpy(&op.coef[2], g.b, 16);
-                std::memcpy(&op.coef[4], g.c, 16);
-                std::memcpy(&op.coef[6], g.d, 16);
-                if (gi.slot >= 0 && (gi.slot & kSlotBranch)) {
-                    // noise branch: per-state coefficients, tested at run time
-                    op.flags = kOpTable | kOpBranch;
-                    op.reserved = (uint32_t)(gi.slot & (kSlotBranch - 1));
-                    op.code = OP_MATRIX;
-                    op.reg = (int8_t)reg_of_local[local_of[g.target]];
-                } else if (gi.slot >= 0) {
-                    // per-state coefficients: generic op reading the batch table
-                    op.flags = kOpTable;
-                    op.reserved = (uint32_t)gi.slot;
-                    if (gi.diag) {
-                        int lt = local_of[g.target];
-                        op.code = OP_DIAG;
-                        op.local = (int8_t)lt;
-                        op.target_outer = lt >= 0 ? 0u : (1u << g.target);
-                    } else {
-                        bool real = g.a[1] == 0 && g.b[1] == 0 && g.c[1] == 0 && g.d[1] == 0;
-                        op.code = real ? OP_MATRIX_REAL : OP_MATRIX;
-                        op.reg = (int8_t)reg_of_local[local_of[g.target]];
-                    }
-                } else if (gi.diag) {
-                    bool a1 = is_exact(g.a, 1.0, 0.0), d1 = is_exact(g.d, 1.0, 0.0);
-                    int lt = local_of[g.target];
-                    if (a1 && is_exact(g.d, -1.0, 0.0)) {
-                        op.code = OP_NEGATE;
-                        if (lt >= 0) op.cmask_local |= (uint16_t)(1u << lt);
-                        else op.cmask_outer |= 1u << g.target;
-                    } else {
-                        op.code = OP_DIAG;
-                        op.local = (int8_t)lt;
-                        op.target_outer = lt >= 0 ? 0u : (1u << g.target);
-                        op.flags = (uint16_t)((a1 ? 1 : 0) | (d1 ? 2 : 0));
-                    }
-                } else if (g.kernel == QM_KERNEL_EXCHANGE) {
-                    op.code = OP_EXCHANGE;
-                    op.reg = (int8_t)reg_of_local[local_of[g.target]];
-                    for (int q = 0; q < qubits && op.reg2 < 0; ++q)
-                        if ((g.control_mask & (1u << q)) && local_of[q] >= 0 && reg_of_local[local_of[q]] >= 0)
-                            op.reg2 = (int8_t)reg_of_local[local_of[q]];
-                } else if (g.kernel == QM_KERNEL_SWAP) {
-                    op.code = OP_SWAP;
-                    op.reg = (int8_t)reg_of_local[local_of[g.target]];
-                    op.reg2 = (int8_t)reg_of_local[local_of[g.swap_control]];
-                } else {
-                    bool real = g.a[1] == 0 && g.b[1] == 0 && g.c[1] == 0 && g.d[1] == 0;
-                    op.code = real ? OP_MATRIX_REAL : OP_MATRIX;
-                    op.reg = (int8_t)reg_of_local[local_of[g.target]];
-                }
-                if ((op.code == OP_MATRIX || op.code == OP_MATRIX_REAL || op.code == OP_EXCHANGE) && op.reg < 0) {
-                    error = "planner placed a gate outside the register layout";
-                    return false;
-                }
-                if (op.code == OP_SWAP && (op.reg < 0 || op.reg2 < 0)) {
-                    error = "planner placed a swap outside the register layout";
-                    return false;
-                }
-                const bool groupable =
-                    (op.code == OP_DIAG && op.cmask_local == 0 && op.cmask_outer == 0) ||
-                    (op.code == OP_NEGATE && popc(op.cmask_local) + popc(op.cmask_outer) <= 2);
-                if (groupable) {
-                    group.push_back(op);
-                    group_qubits |= gi.touch;
-                    continue;
-                }
-                if (!gi.diag && (gi.xmask & group_qubits)) flush();
-                plan.ops.push_back(op);
+                int i = low_bits - 1;
+                while (i >= 0 && idx[i] == nb - low_bits + i) --i;
+                if (i < 0) break;
+                ++idx[i];
+                for (int j = i + 1; j < low_bits; ++j) idx[j] = idx[j - 1] + 1;
             }
-            flush();
+            set_lanes(bestF);
+            place(Q);
         }
-        if (layout & low_local) {
-            emit_stage(canonical);
-            ++stages;
-            set_regs(pass.reg_out, canonical);
-        } else {
-            set_regs(pass.reg_out, layout);
-        }
-        pass.op_count = (int32_t)plan.ops.size() - pass.op_begin;
-        if (pass.op_count > kMaxPassOps) {
-            error = "pass program exceeds the kernel-parameter capacity";
-            return false;
-        }
-        pass.stages = stages;
-        plan.passes.push_back(pass);
-        plan.planned_bytes += 2 * n * elem;
+        if (!build_pass(Q, absorbed)) return false;
+        if (relabel) apply(rest);
         remaining.swap(rest);
+    }
+    if (relabel) {
+        std::vector<GInfo> none;
+        for (int round = 0; !in_order(); ++round) {
+            if (round >= 2 * qubits) {
+                error = "planner could not put the qubits back in order";
+                return false;
+            }
+            uint32_t Q = restoring_block(low_mask);
+            for (int q = 0; q < qubits && popc(Q) < k; ++q) Q |= 1u << q;
+            uint32_t F = 0;
+            for (int b = 0; b < qubits; ++b)
+                if (at[b] < low_bits) F |= 1u << b;
+            set_lanes(F);
+            place(Q);
+            if (!build_pass(Q, none)) return false;
+            apply(none);
+        }
     }
     plan.launches = (int32_t)plan.passes.size();
     return true;

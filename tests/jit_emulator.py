@@ -33,7 +33,7 @@ class Launch(C.Structure):  # FusedLaunch
                 ("op_count", C.c_int32), ("reg_in_g", C.c_uint32 * R), ("reg_out_g", C.c_uint32 * R),
                 ("reg_in_l", C.c_int32 * R), ("cta_shift", C.c_int32), ("states", C.c_int32),
                 ("table_slots", C.c_int32), ("pad", C.c_int32), ("ops", C.c_void_p), ("table", C.c_void_p),
-                ("state_stride", C.c_uint64), ("table_stride", C.c_uint64)]
+                ("state_stride", C.c_uint64), ("table_stride", C.c_uint64), ("out_bit", C.c_uint8 * 16)]
 
 
 def _build(src: str) -> C.CDLL:
@@ -90,9 +90,11 @@ def run_plan(circuit, precision: int, state: np.ndarray) -> np.ndarray:
         for m in range(R):
             L.reg_in_l[m] = p.reg_in[m]
             L.reg_in_g[m] = 1 << p.qubits[p.reg_in[m]]
-            L.reg_out_g[m] = 1 << p.qubits[p.reg_out[m]]
+            L.reg_out_g[m] = 1 << p.qubits_out[p.reg_out[m]]
         L.thread_in = sum(1 << p.qubits[b] for b in range(k) if b not in reg_in)
-        L.thread_out = sum(1 << p.qubits[b] for b in range(k) if b not in reg_out)
+        L.thread_out = sum(1 << p.qubits_out[b] for b in range(k) if b not in reg_out)
+        for r in range(k - R):
+            L.out_bit[r] = p.out_bit[r]
         L.op_count = p.op_count
         L.ops = C.addressof(ops) + p.op_begin * C.sizeof(FusedOpInfo)
         L.cta_shift = n - k

@@ -3,7 +3,8 @@
 The emulator follows the semantics the fused kernel implements: per pass, every CTA owns
 the amplitudes whose block-qubit bits vary and whose other bits are fixed; ops act on the
 block in order; a stage change only moves data between threads, so it merely changes which
-local bit each register index names.  Comparing the emulated result with the oracle checks
+local bit each register index names.  A relabeling pass writes local bit b to index bit
+qubits_out[b] instead of qubits[b].  Comparing the emulated result with the oracle checks
 the planner (gate placement, reordering, register and mask translation) without a GPU.
 """
 from __future__ import annotations
@@ -27,6 +28,14 @@ def program(qubits: int, precision: int, gates, count: int, width: int):
     _lib.check(lib.qm_plan_program(qubits, precision, gates, count, width, C.byref(np_), passes, np_.value,
                                    C.byref(no), ops, no.value, C.byref(nbytes)))
     return list(passes)[:np_.value], list(ops)[:no.value], nbytes.value
+
+
+def scatter(values: np.ndarray, bits) -> np.ndarray:
+    """bit i of each value moved to bit bits[i]"""
+    out = np.zeros_like(values)
+    for i, b in enumerate(bits):
+        out |= ((values >> i) & 1) << b
+    return out
 
 
 def deposit(values: np.ndarray, mask: int) -> np.ndarray:
@@ -103,6 +112,14 @@ def emulate(state: np.ndarray, qubits: int, passes, ops, reg_bits: int = 4) -> n
             else:
                 raise AssertionError(f"unknown op {op.code}")
         assert layout == list(p.reg_out), "a pass must end in its store layout"
-        assert all(b >= 3 for b in layout), "the store layout keeps the lowest qubits on thread bits"
-        s[idx] = blk
+        q_in = [p.qubits[b] for b in range(k)]
+        q_out = [p.qubits_out[b] for b in range(k)]
+        assert sorted(q_out) == q_in, "a pass writes its tile back to the bits it read"
+        staged = any(op.code == OP_STAGE for op in ops[p.op_begin:p.op_begin + p.op_count])
+        assert q_out == q_in or staged, "a relabeling pass orders its stores after every load (a stage)"
+        assert all(q_out[b] >= 3 for b in layout), "the store layout keeps the lowest index bits on thread bits"
+        threads = [q_out[b] for b in range(k) if b not in layout]
+        out_bit = [p.out_bit[r] for r in range(k - reg_bits)]
+        assert sorted(out_bit) == sorted(threads) and out_bit[:3] == [0, 1, 2], "store ranks cover the thread bits"
+        s[outer[:, None] | scatter(local, q_out)[None, :]] = blk
     return s

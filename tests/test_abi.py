@@ -34,7 +34,7 @@ def test_library_exports_every_declared_entry_point():
     missing = [n for n in sorted(names) if not hasattr(lib, n)]
     assert not missing, missing
     assert names == set(_lib.SIGNATURES), "the ctypes binding covers exactly the header"
-    assert lib.qm_abi_version() == 1
+    assert lib.qm_abi_version() == 2
     limit = re.search(r"#define QM_NOALLOC_MAX_TERMS (\d+)", HEADER.read_text())
     assert limit and int(limit.group(1)) == _lib.NOALLOC_MAX_TERMS
 
@@ -61,7 +61,7 @@ def test_struct_layouts_match_the_header():
     assert C.sizeof(_lib.Gate) == 80
     assert C.sizeof(_lib.PauliTermC) == 24
     assert C.sizeof(_lib.FusedOpInfo) == 88
-    assert C.sizeof(_lib.FusedPassInfo) == 84
+    assert C.sizeof(_lib.FusedPassInfo) == 116
     assert C.sizeof(_lib.Options) == 56
 
 
@@ -119,6 +119,53 @@ def test_planner_handles_controls_and_diagonals_outside_the_block():
     for q in range(12):
         c.Rx(q, 0.1 * q)
     _emulate_against_oracle(c, 9, seed=3)
+
+
+def _layout_after(qubits: int, passes) -> list[int]:
+    """The qubit held at each index bit after the passes (each writes local bit b to qubits_out[b])."""
+    at = list(range(qubits))
+    for p in passes:
+        k = p.block_qubits
+        held = {p.qubits[b]: at[p.qubits[b]] for b in range(k)}
+        for b in range(k):
+            at[p.qubits_out[b]] = held[p.qubits[b]]
+    return at
+
+
+@pytest.mark.parametrize("precision,low", [(0, 3), (1, 4)], ids=["fp64", "fp32"])
+def test_relabeling_plans_restore_the_qubit_order(precision, low):
+    """The 30-qubit brick of depth 40: passes follow the light cone by writing the qubits the
+    next pass needs to the lowest index bits, and the last passes put every qubit back.  Every
+    pass writes its tile to the bits it read; its store keeps the coalesced run (the lowest
+    index bits) on the lowest thread ranks."""
+    c = brick_circuit(30, 40)
+    gates, count = prepare(c)
+    passes, ops, planned = pe.program(30, precision, gates, count, 0)
+    assert len(passes) <= (32 if precision == 0 else 36)  # 55 and 62 without relabeling
+    assert planned == len(passes) * 2 * ((8 if precision == 1 else 16) << 30)
+    assert _layout_after(30, passes) == list(range(30))
+    relabeled = 0
+    for p in passes:
+        k = p.block_qubits
+        q = [p.qubits[b] for b in range(k)]
+        q_out = [p.qubits_out[b] for b in range(k)]
+        assert sorted(q_out) == q and q[:low] == list(range(low))
+        assert [p.out_bit[r] for r in range(low)] == list(range(low))
+        # a stage's barriers order the stores of one thread after the loads of every other
+        assert q_out == q or any(o.code == 0 for o in ops[p.op_begin:p.op_begin + p.op_count])
+        relabeled += q_out != q
+    assert relabeled >= len(passes) // 2
+
+
+def test_relabeling_plan_matches_the_oracle_when_emulated():
+    from test_jit_emulated import frame_mix
+    c = frame_mix(18, 6, 11)
+    gates, count = prepare(c)
+    passes, ops, _ = pe.program(18, 0, gates, count, 0)
+    assert any(p.qubits_out[b] != p.qubits[b] for p in passes for b in range(p.block_qubits))
+    psi = random_state(18, 4)
+    got = pe.emulate(psi, 18, passes, ops)
+    assert np.max(np.abs(got - orc.execute(c, psi))) <= 1e-12
 
 
 def test_planner_brick_circuit_pass_counts_and_bytes():

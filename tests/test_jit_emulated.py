@@ -46,10 +46,25 @@ CASES = [
     ("brick_fp64", lambda: brick_circuit(14, 10, seed=8), FP64, 1e-12),
     ("brick_fp32", lambda: brick_circuit(14, 10, seed=9), FP32, 2e-5),
     ("frame_mix", lambda: frame_mix(13, 5, 11), FP64, 1e-12),
+    ("frame_mix_relabeled", lambda: frame_mix(14, 5, 11), FP64, 1e-12),
     ("random", lambda: random_circuit(12, 250, seed=21), FP64, 1e-12),
     ("diagonal", lambda: diagonal_heavy_circuit(12, 250, seed=22), FP64, 1e-12),
     ("qft", lambda: QuantumFourierTransform.CreateCircuit(13), FP64, 1e-12),
 ]
+
+
+def test_cases_reach_relabeling_passes():
+    """The 14-qubit cases plan passes that write qubits to other index bits (pending phases are
+    carried through the relabeling) and stages that set the store lanes."""
+    from quantummatter_b200.circuit import prepare
+    from plan_emulator import program
+    for make, precision in ((lambda: brick_circuit(14, 10, seed=8), FP64), (lambda: brick_circuit(14, 10, seed=9), FP32),
+                            (lambda: frame_mix(14, 5, 11), FP64)):
+        c = make()
+        g, n = prepare(c)
+        passes, ops, _ = program(c.QubitCount, precision, g, n, 0)
+        assert any(p.qubits_out[b] != p.qubits[b] for p in passes for b in range(p.block_qubits))
+        assert any(o.code == 0 and o.reserved for o in ops)
 
 
 @pytest.mark.parametrize("name,make,precision,tol", CASES, ids=[c[0] for c in CASES])
