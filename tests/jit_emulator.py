@@ -65,24 +65,25 @@ def _text(fn, *args) -> bytes:
     return buf.raw[:ln.value]
 
 
-def run_plan(circuit, precision: int, state: np.ndarray) -> np.ndarray:
-    """The plan's compiled passes applied to a copy of `state` on the CPU."""
+def run_plan(circuit, precision: int, state: np.ndarray, width: int = 0) -> np.ndarray:
+    """The plan's compiled passes (fusion width `width`, 0: the default) applied to a copy of
+    `state` on the CPU."""
     n = circuit.QubitCount
     g, count = prepare(circuit)
     lib = load()
     P, O, pb = C.c_int32(), C.c_int32(), C.c_int64()
-    check(lib.qm_plan_program(n, precision, g, count, 0, C.byref(P), None, 0, C.byref(O), None, 0, C.byref(pb)))
+    check(lib.qm_plan_program(n, precision, g, count, width, C.byref(P), None, 0, C.byref(O), None, 0, C.byref(pb)))
     passes = (FusedPassInfo * max(1, P.value))()
     ops = (FusedOpInfo * max(1, O.value))()
-    check(lib.qm_plan_program(n, precision, g, count, 0, C.byref(P), passes, P.value, C.byref(O), ops, O.value,
+    check(lib.qm_plan_program(n, precision, g, count, width, C.byref(P), passes, P.value, C.byref(O), ops, O.value,
                               C.byref(pb)))
     s = np.array(state, dtype=np.complex64 if precision == FP32 else np.complex128, copy=True)
     all_mask = (1 << n) - 1
     for i in range(P.value):
         p = passes[i]
         k = p.block_qubits
-        src = _text(lib.qm_jit_source, n, precision, g, count, 0, i).decode()
-        aux = _text(lib.qm_jit_constants, n, precision, g, count, 0, i)
+        src = _text(lib.qm_jit_source, n, precision, g, count, width, i).decode()
+        aux = _text(lib.qm_jit_constants, n, precision, g, count, width, i)
         L = Launch()
         L.outer_mask = all_mask & ~p.block_mask
         reg_in = {p.reg_in[m] for m in range(R)}

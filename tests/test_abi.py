@@ -157,6 +157,19 @@ def test_relabeling_plans_restore_the_qubit_order(precision, low):
     assert relabeled >= len(passes) // 2
 
 
+@pytest.mark.parametrize("precision,width", [(0, 9), (0, 10), (0, 11), (1, 9), (1, 11), (1, 13)])
+def test_relabeling_plans_match_the_oracle_at_every_block_width(precision, width):
+    """Explicit fusion widths plan relabeling passes too (lanes of 3 bits in FP64, 4 in FP32)."""
+    c = random_circuit(16, 300, seed=9)
+    gates, count = prepare(c)
+    passes, ops, _ = pe.program(16, precision, gates, count, width)
+    assert all(p.block_qubits == width for p in passes)
+    assert any(p.qubits_out[b] != p.qubits[b] for p in passes for b in range(p.block_qubits))
+    psi = random_state(16, 1)
+    got = pe.emulate(psi, 16, passes, ops)
+    assert np.max(np.abs(got - orc.execute(c, psi))) <= 1e-12
+
+
 def test_relabeling_plan_matches_the_oracle_when_emulated():
     from test_jit_emulated import frame_mix
     c = frame_mix(18, 6, 11)

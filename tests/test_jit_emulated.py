@@ -53,6 +53,23 @@ CASES = [
 ]
 
 
+@pytest.mark.parametrize("precision,width,tol", [(FP64, 9, 1e-12), (FP32, 13, 2e-5)], ids=["fp64-k9", "fp32-k13"])
+def test_relabeling_passes_at_other_block_widths(precision, width, tol):
+    """Generated kernels of relabeling plans with 9-qubit blocks (32 threads) and 13-qubit blocks
+    (512 threads, complex64 only): lane codes and permuted stores at both ends of the range."""
+    from quantummatter_b200.circuit import prepare
+    from plan_emulator import program
+    c = random_circuit(15, 220, seed=31)
+    g, n = prepare(c)
+    passes, ops, _ = program(15, precision, g, n, width)
+    assert any(p.qubits_out[b] != p.qubits[b] for p in passes for b in range(p.block_qubits))
+    assert any(o.code == 0 and o.reserved for o in ops)
+    psi = random_state(15, 2)
+    want = orc.execute(c, psi)
+    got = je.run_plan(c, precision, psi, width)
+    assert np.max(np.abs(got - want)) <= tol
+
+
 def test_cases_reach_relabeling_passes():
     """The 14-qubit cases plan passes that write qubits to other index bits (pending phases are
     carried through the relabeling) and stages that set the store lanes."""
