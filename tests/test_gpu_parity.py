@@ -301,6 +301,27 @@ def test_measure_all_collapses_like_the_oracle(gpu_context):
         assert np.array_equal(got, want_state)
 
 
+@pytest.mark.parametrize("precision,width,tol", [(FP64, 9, 1e-12), (FP64, 11, 1e-12), (FP32, 13, 2e-5)],
+                         ids=["fp64-k9", "fp64-k11", "fp32-k13"])
+def test_relabeling_plans_at_other_block_widths(gpu_context, precision, width, tol):
+    """Relabeling passes at explicit fusion widths: one-shot (the interpreter runs passes not yet
+    compiled) and as a compiled plan, against the oracle."""
+    c = random_circuit(20, 400, seed=41)
+    psi = random_state(20, 3)
+    want = orc.execute(c, psi)
+    for compiled in (False, True):
+        with DeviceState(gpu_context, 20, precision) as st:
+            st.Upload(psi)
+            if compiled:
+                p = Plan(gpu_context, c, precision, width)
+                p.execute(st)
+                p.Dispose()
+            else:
+                st.Evolve(c, fusion_width=width)
+            got = st.Download()
+        assert np.max(np.abs(got - want)) <= tol, (compiled, width)
+
+
 @pytest.mark.parametrize("n", [21, 24])
 def test_pageable_host_buffers_match_page_locked_ones(gpu_context, n):
     """Whole-state copies from pageable host memory of 16 MiB and more move through the
