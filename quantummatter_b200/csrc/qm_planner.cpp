@@ -13,6 +13,9 @@
 //   * a gate may move ahead of a skipped gate only if they commute.
 // Diagonal gates never need block or register space: their phase is a function of the
 // global index, which every amplitude knows.
+// Plans without per-state coefficients also relabel qubits: a pass may write its block back
+// with the qubits permuted among the block's index bits, so that the lowest bits (the run every
+// pass reads whole) hold the qubits the next pass can use best; the last passes restore the order.
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
