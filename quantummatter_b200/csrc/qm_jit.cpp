@@ -924,13 +924,15 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int
     // partial row u = state * rows + r always holds the same tiles [r C, (r + 1) C) of its state
     // (rows = 2^(n-16), the layout of launch_group_histogram), whatever the state's place in the
     // batch.  Within a chunk the bins accumulate per warp in shared memory in a fixed order.
-    // a relabeling pass (qubits written to other bits, lanes in a stage) keeps the separate
-    // joint-mass kernel: the epilogue reads the bins in the unpermuted, ascending layout
+    // a relabeling pass (qubits written to other bits, lanes in the store layout) keeps the
+    // separate joint-mass kernel: the epilogue reads the bins in the unpermuted, ascending layout
     bool relabels = false;
     for (int b = 0; b < p.k; ++b) relabels |= p.q_out[b] != p.q[b];
-    for (int o = 0; o < p.op_count; ++o) {
+    for (int o = p.op_count - 1; o >= 0; --o) {
         const FusedOp& op = plan_ops[(size_t)(p.op_begin + o)];
-        relabels |= op.code == OP_STAGE && op.reserved != 0;
+        if (op.code != OP_STAGE) continue;
+        relabels |= op.reserved != 0;  // the last stage sets the store layout
+        break;
     }
     const bool hist = hist_mask != 0 && __builtin_popcount(hist_mask) <= kGroupMaxBits && !relabels;
     const int hist_bins = hist ? 1 << __builtin_popcount(hist_mask) : 0;

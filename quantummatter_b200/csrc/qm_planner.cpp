@@ -469,6 +469,42 @@ bool plan_fused(const std::vector<qm_gate>& gates, int qubits, int precision, in
                 }
             }
             {
+                // Exchanges go through shared memory in phases of 2^low_bits threads (thread ranks
+                // 0..low_bits-1 vary), and the swizzle sends local bit p to bank-group bit
+                // p mod low_bits: an exchange side is free of bank conflicts when those ranks
+                // hold bits of distinct classes.  The load layout holds bits 0..low_bits-1 there
+                // and the last stage's ranks are fixed by the store, so every other stage whose
+                // ascending ranks collide takes lanes of distinct classes when its free bits have
+                // them.
+                int last_stage = -1;
+                for (size_t o = (size_t)pass.op_begin; o < plan.ops.size(); ++o)
+                    if (plan.ops[o].code == OP_STAGE) last_stage = (int)o;
+                for (size_t o = (size_t)pass.op_begin; (int)o < last_stage; ++o) {
+                    FusedOp& st = plan.ops[o];
+                    if (st.code != OP_STAGE || st.reserved != 0) continue;
+                    uint32_t regs = 0;
+                    for (int m = 0; m < kRegBits; ++m) regs |= 1u << st.reg_pos[m];
+                    uint32_t seen = 0;
+                    int n = 0;
+                    for (int b = 0; b < k && n < low_bits; ++b)
+                        if (!(regs & (1u << b))) {
+                            seen |= 1u << (b % low_bits);
+                            ++n;
+                        }
+                    if (seen == (1u << low_bits) - 1u) continue;  // ascending ranks are conflict-free
+                    uint32_t code = (uint32_t)low_bits;
+                    bool found = true;
+                    for (int c = 0; c < low_bits && found; ++c) {
+                        int pick = -1;
+                        for (int b = c; b < k && pick < 0; b += low_bits)
+                            if (!(regs & (1u << b))) pick = b;
+                        if (pick < 0) found = false;
+                        else code |= (uint32_t)pick << (4 + 4 * c);
+                    }
+                    if (found) st.reserved = code;
+                }
+            }
+            {
                 // store order: the lanes (when given), then the other thread bits ascending
                 int rank = 0;
                 if (lanes_needed)
@@ -632,9 +668,14 @@ bool plan_fused(const std::vector<qm_gate>& gates, int qubits, int precision, in
             int idx[8];
             for (int i = 0; i < low_bits; ++i) idx[i] = i;
             while (true) {
-                uint32_t F = 0;
-                for (int i = 0; i < low_bits; ++i) F |= 1u << bits[idx[i]];
-                const int score = 2 * absorbable(F) + (F == low_mask ? 1 : 0);
+                uint32_t F = 0, classes = 0;
+                for (int i = 0; i < low_bits; ++i) {
+                    F |= 1u << bits[idx[i]];
+                    classes |= 1u << (idx[i] % low_bits);  // idx[i] is the local bit
+                }
+                // ties go to lanes of distinct bank-group classes (a conflict-free last exchange),
+                // then to keeping the layout
+                const int score = 4 * absorbable(F) + (classes == (1u << low_bits) - 1u ? 2 : 0) + (F == low_mask ? 1 : 0);
                 if (score > best) {
                     best = score;
                     bestF = F;
