@@ -157,6 +157,38 @@ def test_relabeling_plans_restore_the_qubit_order(precision, low):
     assert relabeled >= len(passes) // 2
 
 
+def _lowest_ranks(registers, lanes, k, n):
+    free = [b for b in range(k) if b not in registers and b not in lanes]
+    return (list(lanes) + free)[:n]
+
+
+@pytest.mark.parametrize("precision,low,allowed", [(0, 3, 0.0), (1, 4, 0.1)], ids=["fp64", "fp32"])
+def test_exchanges_keep_shared_memory_free_of_bank_conflicts(precision, low, allowed):
+    """An exchange goes through shared memory in phases of 2^low threads (ranks 0..low-1) and the
+    swizzle sends local bit p to bank-group bit p mod low: every exchange side but a relabeling
+    pass's final lanes (fixed by the store) holds bits of distinct classes on those ranks
+    (complex64 stages may lack a class among their free bits)."""
+    c = brick_circuit(30, 40)
+    gates, count = prepare(c)
+    passes, ops, _ = pe.program(30, precision, gates, count, 0)
+    sides = colliding = 0
+    for p in passes:
+        k = p.block_qubits
+        registers, lanes = list(p.reg_in), []
+        stages = [o for o in ops[p.op_begin:p.op_begin + p.op_count] if o.code == 0]
+        for i, o in enumerate(stages):
+            new_lanes = [(o.reserved >> (4 + 4 * r)) & 15 for r in range(o.reserved & 15)]
+            checked = [(registers, lanes)]
+            if i < len(stages) - 1:  # the last stage's read side holds the store's ranks
+                checked.append((list(o.reg_pos), new_lanes))
+            for regs, ln in checked:
+                ranks = _lowest_ranks(regs, ln, k, low)
+                sides += 1
+                colliding += len({b % low for b in ranks}) < low
+            registers, lanes = list(o.reg_pos), new_lanes
+    assert sides > 100 and colliding <= allowed * sides, (colliding, sides)
+
+
 @pytest.mark.parametrize("precision,width", [(0, 9), (0, 10), (0, 11), (1, 9), (1, 11), (1, 13)])
 def test_relabeling_plans_match_the_oracle_at_every_block_width(precision, width):
     """Explicit fusion widths plan relabeling passes too (lanes of 3 bits in FP64, 4 in FP32)."""
