@@ -74,15 +74,6 @@ int32_t ensure_host_scratch(qm_context* ctx, size_t bytes) {
     return QM_OK;
 }
 
-bool is_pinned(const void* p) {
-    cudaPointerAttributes attr;
-    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
-    }
-    return attr.type == cudaMemoryTypeHost;
-}
-
 // ---------------------------------------------------------------- gate preparation
 
 // Builder validation (src/QuantumMatter.Core/QuantumCircuit.cs:97-134).
