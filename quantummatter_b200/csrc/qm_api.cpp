@@ -259,8 +259,10 @@ int32_t build_plan(qm_context* ctx, int32_t qubits, int32_t precision, const qm_
     if (width == 0) width = ctx->fusion_width;
     if (!plan_fused(list, qubits, precision, width, plan, err)) return fail(QM_E_ARG, "planner: " + err);
     // one-shot executions of large states run the compiled passes already built for the same
-    // structures; they never wait for a compilation
-    if (transient && qubits >= 20) jit_lookup(plan);
+    // structures; they never wait for a compilation.  Below 26 qubits a pass takes well under a
+    // millisecond, about what generating the plan's sources for the lookup costs on the host,
+    // so those run the interpreter.
+    if (transient && qubits >= 26) jit_lookup(plan);
     if (transient) return plan_upload(plan, ctx->stream, &ctx->program, &ctx->program_bytes);
     return plan_upload(plan, ctx->stream);
 }

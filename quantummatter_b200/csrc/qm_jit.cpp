@@ -1199,6 +1199,7 @@ struct Entry {
 };
 
 std::mutex g_cache_mu;
+std::atomic<bool> g_self_contained{false};  // some plan compiled self-contained passes
 std::unordered_map<std::string, Entry> g_cache;
 std::atomic<int64_t> g_compiled{0}, g_failed{0}, g_launches{0};
 
@@ -1336,6 +1337,7 @@ void jit_prepare(Plan& plan) {
     }
     gen = generate_plan(plan, false);
     compile_all(gen);
+    g_self_contained.store(true);
     install(plan, gen, false);
 }
 
@@ -1356,6 +1358,9 @@ void jit_lookup(Plan& plan) {
         install(plan, gen, true);
         return;
     }
+    // self-contained passes are only compiled when a chained plan failed to; until then there
+    // is nothing to find and the generation (about a millisecond per plan) is skipped
+    if (!g_self_contained.load()) return;
     gen = generate_plan(plan, false);
     install(plan, gen, true);
 }
