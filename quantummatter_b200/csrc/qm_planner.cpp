@@ -16,6 +16,7 @@
 // Plans without per-state coefficients also relabel qubits: a pass may write its block back
 // with the qubits permuted among the block's index bits, so that the lowest bits (the run every
 // pass reads whole) hold the qubits the next pass can use best; the last passes restore the order.
+// Such a plan is kept only when it needs fewer passes than the plain one.
 #include <algorithm>
 #include <cstdlib>
 #include <cstring>
@@ -105,8 +106,18 @@ int default_block_qubits(int qubits, int precision) {
     return std::min(12, qubits);
 }
 
-bool plan_fused(const std::vector<qm_gate>& gates, int qubits, int precision, int width, Plan& plan,
-                std::string& error, const std::vector<int32_t>* slots) {
+namespace {
+
+bool relabel_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("QM_RELABEL");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
+bool plan_fused_with(const std::vector<qm_gate>& gates, int qubits, int precision, int width, Plan& plan,
+                     std::string& error, const std::vector<int32_t>* slots, bool allow_relabel) {
     plan.qubits = qubits;
     plan.precision = precision;
     plan.passes.clear();
@@ -180,11 +191,7 @@ bool plan_fused(const std::vector<qm_gate>& gates, int qubits, int precision, in
     // renamed to match.  Blocks then follow the circuit's light cone instead of carrying qubits
     // 0..low_bits-1 through every pass.  `at[b]` is the qubit held at index bit b; the last
     // passes put every qubit back at its own bit.
-    static const bool relabel_env = [] {
-        const char* e = std::getenv("QM_RELABEL");
-        return !(e && e[0] == '0');
-    }();
-    const bool relabel = relabel_env && !slots && qubits > k;
+    const bool relabel = allow_relabel && !slots && qubits > k;
     const uint32_t all_qubits = qubits >= 32 ? 0xffffffffu : (1u << qubits) - 1u;
     int at[32];
     for (int q = 0; q < 32; ++q) at[q] = q;
@@ -712,6 +719,23 @@ bool plan_fused(const std::vector<qm_gate>& gates, int qubits, int precision, in
         }
     }
     plan.launches = (int32_t)plan.passes.size();
+    return true;
+}
+
+}  // namespace
+
+// Plans without relabeling and, where relabeling applies, with it: the relabeling plan is kept
+// only when it needs fewer passes, since its lane stages and restoring pass cost more than they
+// save otherwise.
+bool plan_fused(const std::vector<qm_gate>& gates, int qubits, int precision, int width, Plan& plan,
+                std::string& error, const std::vector<int32_t>* slots) {
+    if (!plan_fused_with(gates, qubits, precision, width, plan, error, slots, false)) return false;
+    if (slots || !relabel_enabled() || plan.width == 1 || plan.passes.size() < 2) return true;
+    Plan alt;
+    std::string alt_error;
+    if (plan_fused_with(gates, qubits, precision, width, alt, alt_error, slots, true) &&
+        alt.passes.size() < plan.passes.size())
+        plan = std::move(alt);
     return true;
 }
 

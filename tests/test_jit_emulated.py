@@ -46,7 +46,8 @@ CASES = [
     ("brick_fp64", lambda: brick_circuit(14, 10, seed=8), FP64, 1e-12),
     ("brick_fp32", lambda: brick_circuit(14, 10, seed=9), FP32, 2e-5),
     ("frame_mix", lambda: frame_mix(13, 5, 11), FP64, 1e-12),
-    ("frame_mix_relabeled", lambda: frame_mix(14, 5, 11), FP64, 1e-12),
+    ("random_relabeled_fp64", lambda: random_circuit(14, 400, seed=14), FP64, 1e-12),
+    ("random_relabeled_fp32", lambda: random_circuit(14, 400, seed=14), FP32, 2e-5),
     ("random", lambda: random_circuit(12, 250, seed=21), FP64, 1e-12),
     ("diagonal", lambda: diagonal_heavy_circuit(12, 250, seed=22), FP64, 1e-12),
     ("qft", lambda: QuantumFourierTransform.CreateCircuit(13), FP64, 1e-12),
@@ -59,24 +60,25 @@ def test_relabeling_passes_at_other_block_widths(precision, width, tol):
     (512 threads, complex64 only): lane codes and permuted stores at both ends of the range."""
     from quantummatter_b200.circuit import prepare
     from plan_emulator import program
-    c = random_circuit(15, 220, seed=31)
+    c = random_circuit(16, 400, seed=16)
     g, n = prepare(c)
-    passes, ops, _ = program(15, precision, g, n, width)
+    passes, ops, _ = program(16, precision, g, n, width)
     assert any(p.qubits_out[b] != p.qubits[b] for p in passes for b in range(p.block_qubits))
     assert any(o.code == 0 and o.reserved for o in ops)
-    psi = random_state(15, 2)
+    psi = random_state(16, 2)
     want = orc.execute(c, psi)
     got = je.run_plan(c, precision, psi, width)
     assert np.max(np.abs(got - want)) <= tol
 
 
 def test_cases_reach_relabeling_passes():
-    """The 14-qubit cases plan passes that write qubits to other index bits (pending phases are
-    carried through the relabeling) and stages that set the store lanes."""
+    """The relabeled cases plan passes that write qubits to other index bits (pending phases are
+    carried through the relabeling) and stages that set the store lanes: the planner keeps
+    relabeling there because it saves passes."""
     from quantummatter_b200.circuit import prepare
     from plan_emulator import program
-    for make, precision in ((lambda: brick_circuit(14, 10, seed=8), FP64), (lambda: brick_circuit(14, 10, seed=9), FP32),
-                            (lambda: frame_mix(14, 5, 11), FP64)):
+    for make, precision in ((lambda: random_circuit(14, 400, seed=14), FP64),
+                            (lambda: random_circuit(14, 400, seed=14), FP32)):
         c = make()
         g, n = prepare(c)
         passes, ops, _ = program(c.QubitCount, precision, g, n, 0)
