@@ -157,6 +157,33 @@ def test_relabeling_plans_restore_the_qubit_order(precision, low):
     assert relabeled >= len(passes) // 2
 
 
+def test_relabeling_is_kept_only_where_it_saves_passes():
+    """A 14-qubit brick of depth 10 needs 3 passes either way: it keeps the plain plan (no lane
+    stages, no restoring pass).  The 30-qubit brick of depth 40 keeps its relabeling plan, and a
+    subprocess with QM_RELABEL=0 shows the plain plan it replaced."""
+    import json
+    import os
+    import subprocess
+    import sys
+
+    def counts(c, precision=0):
+        gates, count = prepare(c)
+        passes, ops, _ = pe.program(c.QubitCount, precision, gates, count, 0)
+        relabels = any(p.qubits_out[b] != p.qubits[b] for p in passes for b in range(p.block_qubits))
+        return len(passes), relabels
+
+    assert counts(brick_circuit(14, 10, seed=8)) == (3, False)
+    relabeled, relabels = counts(brick_circuit(30, 40))
+    assert relabels
+    script = ("import json, sys; sys.path[:0] = ['tests', 'oracle']; import plan_emulator as pe; "
+              "from quantummatter_b200.circuit import prepare; from quantummatter_b200.workloads import brick_circuit; "
+              "g, n = prepare(brick_circuit(30, 40)); print(json.dumps(len(pe.program(30, 0, g, n, 0)[0])))")
+    out = subprocess.run([sys.executable, "-c", script], cwd=ROOT, capture_output=True, text=True, timeout=300,
+                         env={**os.environ, "QM_RELABEL": "0"})
+    assert out.returncode == 0, out.stderr[-2000:]
+    assert relabeled < json.loads(out.stdout.strip().splitlines()[-1])
+
+
 def _lowest_ranks(registers, lanes, k, n):
     free = [b for b in range(k) if b not in registers and b not in lanes]
     return (list(lanes) + free)[:n]
