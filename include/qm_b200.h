@@ -459,10 +459,14 @@ int32_t qm_random_doubles(int32_t seed, int64_t skip, int64_t count, double* out
  *
  * It allocates nothing: its scratch (the reduction's per-block partial sums) is a fixed
  * file-scope device array of about 304 KB per device, zeroed by the call itself.  The first
- * call on each device looks that array's address up (cudaGetSymbolAddress); make that first
- * call before any stream capture begins.  count > QM_NOALLOC_MAX_TERMS gives QM_E_RANGE.
- * Calls whose work can overlap on one GPU (from several host threads, or on several streams)
- * race on that device's scratch and give wrong sums: serialise them. */
+ * call on each device looks that array's address up (cudaGetSymbolAddress).  CUDA loads a
+ * library's device code lazily, so that first call also loads the modules holding the array
+ * and the kernels, which reserves about 304 KB plus their code on the device: a host whose pool
+ * takes the GPU's memory makes one warm-up call (count = 0 is enough) before the pool does, and
+ * before any stream capture begins.  The address is cached for the life of the process, so the
+ * entry point must not be used across a cudaDeviceReset.  count > QM_NOALLOC_MAX_TERMS gives
+ * QM_E_RANGE.  Calls whose work can overlap on one GPU (from several host threads, or on
+ * several streams) race on that device's scratch and give wrong sums: serialise them. */
 #define QM_NOALLOC_MAX_TERMS 64
 int32_t qm_expectation_pauli_noalloc(const void* amplitudes, int32_t qubits, int32_t precision,
                                      const qm_pauli_term* terms, int32_t count, double* per_term,

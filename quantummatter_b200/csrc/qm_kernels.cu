@@ -490,7 +490,7 @@ cudaError_t launch_convert_to_f64(double* dst, const void* src, int64_t n, cudaS
 
 static int reduce_blocks(uint64_t items) {
     uint64_t b = (items + kThreads * 8 - 1) / (kThreads * 8);
-    return (int)std::max<uint64_t>(1, std::min<uint64_t>(b, 148ull * 4));
+    return (int)std::max<uint64_t>(1, std::min<uint64_t>(b, (uint64_t)kReduceBlocksMax));
 }
 
 cudaError_t launch_masses(const void* amps, int qubits, int precision, int target, double* scratch, int* blocks_out,

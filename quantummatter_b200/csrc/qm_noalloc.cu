@@ -24,7 +24,8 @@ namespace {
 
 constexpr int kMaxTerms = QM_NOALLOC_MAX_TERMS;
 constexpr int kColumns = kMaxTerms + 1;  // the Born mass rides in the last column
-constexpr int kMaxBlocks = 592;          // expectation_blocks() never returns more
+constexpr int kMaxBlocks = kReduceBlocksMax;  // expectation_blocks() never returns more
+static_assert(kMaxBlocks >= 1 && kMaxBlocks <= 4096, "the fixed scratch is sized from the reduction grid cap");
 constexpr size_t kScratchDoubles = (size_t)(kMaxBlocks + 1) * kColumns;
 constexpr int kMaxDevices = 64;
 
@@ -38,7 +39,10 @@ double* g_address[kMaxDevices] = {};
 
 // Device address of g_scratch on the current device, looked up once per device.  In host
 // code `g_scratch` names a host-side stand-in, not device memory, so the kernels get this
-// address instead.
+// address instead.  The address is cached for the life of the process: a cudaDeviceReset by
+// the host unloads the module that holds the array, so the entry point must not be used across
+// one.  The first lookup also loads that module (CUDA loads modules lazily), which reserves the
+// array's memory on the device.
 int32_t scratch_address(double** out) {
     int device = 0;
     cudaError_t e = cudaGetDevice(&device);
@@ -74,6 +78,8 @@ extern "C" int32_t qm_expectation_pauli_noalloc(const void* amplitudes, int32_t 
     if (rc) return rc;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const int blocks = expectation_blocks(qubits);
+    if (blocks < 1 || blocks > kMaxBlocks)
+        return fail(QM_E_RANGE, "the reduction grid exceeds the fixed scratch of qm_expectation_pauli_noalloc");
     const int columns = count + 1;
     double* partials = scratch;                            // [blocks][columns]
     double* sums = scratch + (size_t)kMaxBlocks * kColumns; // [columns]

@@ -61,6 +61,22 @@ def test_noalloc_matches_the_allocating_entry_point(gpu_context, precision, qubi
 
 
 @pytest.mark.gpu
+def test_noalloc_reserves_no_device_memory(gpu_context):
+    """After a warm-up call has loaded the modules, calls leave the device's free memory unchanged."""
+    import torch
+    n = 22
+    obs = [PauliString(lab) for lab in labels_for(n, 7, 40)]
+    with DeviceState(gpu_context, n, FP64) as st:
+        st.Evolve(brick_circuit(n, 4, seed=3))
+        noalloc(st, obs)
+        free_before, _ = torch.cuda.mem_get_info(0)
+        for _ in range(3):
+            noalloc(st, obs)
+        free_after, _ = torch.cuda.mem_get_info(0)
+    assert free_after == free_before
+
+
+@pytest.mark.gpu
 def test_noalloc_limits_and_mass_only(gpu_context):
     n = 10
     with DeviceState(gpu_context, n, FP64) as st:
