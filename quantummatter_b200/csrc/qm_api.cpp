@@ -219,6 +219,20 @@ int32_t validate_prepared_gates(const qm_gate* gates, int32_t count, int32_t qub
 }
 
 int32_t plan_upload(Plan& plan, cudaStream_t stream, void** buffer, size_t* buffer_bytes) {
+    if (!plan.dense.empty() && !plan.d_status) {
+        QM_CUDA(cudaMalloc(&plan.d_status, sizeof(int32_t)));
+        QM_CUDA(cudaMemsetAsync(plan.d_status, 0, sizeof(int32_t), stream));
+        if (!plan.dense_matrices.empty()) {
+            const size_t mbytes = plan.dense_matrices.size() * sizeof(double);
+            QM_CUDA(cudaMalloc(&plan.d_dense, mbytes));
+            QM_CUDA(cudaMemcpyAsync(plan.d_dense, plan.dense_matrices.data(), mbytes, cudaMemcpyHostToDevice, stream));
+        }
+        if (!plan.dense_tc.empty()) {
+            const size_t ibytes = plan.dense_tc.size() * sizeof(float);
+            QM_CUDA(cudaMalloc(&plan.d_dense_tc, ibytes));
+            QM_CUDA(cudaMemcpyAsync(plan.d_dense_tc, plan.dense_tc.data(), ibytes, cudaMemcpyHostToDevice, stream));
+        }
+    }
     if (plan.ops.empty() || plan.d_ops) return QM_OK;
     const size_t bytes = plan.ops.size() * sizeof(FusedOp);
     if (buffer) {
@@ -245,11 +259,33 @@ void plan_release(Plan& plan) {
     if (plan.d_ops && !plan.borrowed) cudaFree(plan.d_ops);  // cudaFree waits for work using the buffer
     plan.d_ops = nullptr;
     plan.borrowed = false;
+    if (plan.d_dense) cudaFree(plan.d_dense);
+    if (plan.d_dense_tc) cudaFree(plan.d_dense_tc);
+    if (plan.d_status) cudaFree(plan.d_status);
+    plan.d_dense = nullptr;
+    plan.d_dense_tc = nullptr;
+    plan.d_status = nullptr;
+}
+
+// After the stream has finished a dense plan: QM_E_TIMEOUT if one of its kernels gave up a wait.
+int32_t dense_status(const Plan& plan) {
+    if (!plan.d_status) return QM_OK;
+    int32_t status = 0;
+    QM_CUDA(cudaMemcpy(&status, plan.d_status, sizeof status, cudaMemcpyDeviceToHost));
+    if (status == 0) return QM_OK;
+    cudaMemset(plan.d_status, 0, sizeof(int32_t));
+    return fail(QM_E_TIMEOUT, "a dense fused-gate kernel gave up waiting for its tile copies");
 }
 
 }  // namespace qm
 
 namespace {
+
+// Fusion widths: 0 = planner default, 1 = one launch per gate, 2..6 = dense fused gates of at
+// most that many qubits, 9..14 = fused blocks of that many qubits.  7 and 8 are neither.
+constexpr const char* kWidthRule =
+    "fusion width must be 0, 1, 2..6 (dense fused gates) or 9..14 (fused blocks)";
+bool valid_width(int32_t w) { return (w >= 0 && w <= kDenseMaxQubits) || (w >= 9 && w <= 14); }
 
 // transient plans (one-shot executions) borrow the context's program buffer
 int32_t build_plan(qm_context* ctx, int32_t qubits, int32_t precision, const qm_gate* gates, int32_t count,
@@ -284,6 +320,20 @@ int32_t run_plan(qm_context* ctx, const Plan& plan, void* amps, const volatile i
     if (plan.width == 1) {
         for (const DevGate& g : plan.gates) {
             QM_CUDA(launch_gate(amps, plan.qubits, plan.precision, g, ctx->stream));
+            int32_t rc = chunk_boundary();
+            if (rc) return rc;
+        }
+    } else if (plan.width <= kDenseMaxQubits) {
+        for (const DenseOp& op : plan.dense) {
+            if (op.m == 0)
+                QM_CUDA(launch_gate(amps, plan.qubits, plan.precision, op.gate, ctx->stream));
+            else if (op.tc_image >= 0)
+                QM_CUDA(launch_dense_tc(amps, plan.qubits, op, plan.d_dense_tc + op.tc_image, plan.d_status,
+                                        ctx->sm_count, ctx->stream));
+            else
+                QM_CUDA(launch_dense(amps, plan.qubits, plan.precision, op,
+                                     reinterpret_cast<const double2*>(plan.d_dense) + op.matrix, plan.d_status,
+                                     ctx->sm_count, ctx->stream));
             int32_t rc = chunk_boundary();
             if (rc) return rc;
         }
@@ -367,7 +417,7 @@ extern "C" int32_t qm_context_create(const qm_options* options, qm_context** out
     if (options) o = *options; else qm_options_default(&o);
     if (o.device_index < 0) return fail(QM_E_RANGE, "device index must be nonnegative");
     if (o.device_budget_bytes < 32 || o.staging_budget_bytes < 32) return fail(QM_E_RANGE, "budgets must be at least 32 bytes");
-    if (o.fusion_width < 0 || o.fusion_width > 14) return fail(QM_E_RANGE, "fusion width must be in [0,14]");
+    if (!valid_width(o.fusion_width)) return fail(QM_E_RANGE, kWidthRule);
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
         cudaGetLastError();
@@ -505,6 +555,7 @@ extern "C" int32_t qm_execute_host(qm_context* ctx, int32_t qubits, const qm_ope
         if (profile) cudaEventRecord(t2, ctx->stream);
         e = cudaStreamSynchronize(ctx->stream);
     }
+    if (e == cudaSuccess && rc == QM_OK) rc = dense_status(plan);
     if (e == cudaSuccess && rc == QM_OK && cancelled(cancel)) rc = fail(QM_E_CANCELLED, "operation cancelled");
     // commit: only after every launch completed and the last cancellation check passed
     if (e == cudaSuccess && rc == QM_OK) {
@@ -758,7 +809,7 @@ extern "C" int32_t qm_plan_create(qm_context* ctx, int32_t qubits, int32_t preci
     *out = nullptr;
     if (qubits < 1 || qubits > 30) return fail(QM_E_RANGE, "qubits must be between 1 and 30");
     if (precision != QM_FP64 && precision != QM_FP32) return fail(QM_E_RANGE, "unknown precision");
-    if (width < 0 || width > 14) return fail(QM_E_RANGE, "fusion width must be in [0,14]");
+    if (!valid_width(width)) return fail(QM_E_RANGE, kWidthRule);
     int32_t rc = validate_gates(gates, count, qubits);
     if (rc) return rc;
     std::lock_guard<std::recursive_mutex> lock(ctx->mu);
@@ -804,7 +855,7 @@ extern "C" int32_t qm_plan_program(int32_t qubits, int32_t precision, const qm_g
                                    int64_t* planned_bytes) {
     if (qubits < 1 || qubits > 30) return fail(QM_E_RANGE, "qubits must be between 1 and 30");
     if (precision != QM_FP64 && precision != QM_FP32) return fail(QM_E_RANGE, "unknown precision");
-    if (width < 0 || width > 14) return fail(QM_E_RANGE, "fusion width must be in [0,14]");
+    if (!valid_width(width)) return fail(QM_E_RANGE, kWidthRule);
     int32_t rc = validate_gates(gates, count, qubits);
     if (rc) return rc;
     Plan plan;
@@ -834,6 +885,8 @@ int32_t execute_plan(qm_state* st, const Plan& plan, qm_profile* profile) {
     }
     if (profile) QM_CUDA(cudaEventRecord(ctx->ev_stop, ctx->stream));
     QM_CUDA(cudaStreamSynchronize(ctx->stream));
+    rc = dense_status(plan);
+    if (rc) return rc;
     if (profile) {
         std::memset(profile, 0, sizeof *profile);
         profile->device_seconds = seconds_between(ctx->ev_start, ctx->ev_stop);
@@ -861,7 +914,7 @@ extern "C" int32_t qm_plan_execute(qm_plan* p, qm_state* st, qm_profile* profile
 extern "C" int32_t qm_execute(qm_state* st, const qm_gate* gates, int32_t count, int32_t width, qm_profile* profile) {
     int32_t rc = check_state(st);
     if (rc) return rc;
-    if (width < 0 || width > 14) return fail(QM_E_RANGE, "fusion width must be in [0,14]");
+    if (!valid_width(width)) return fail(QM_E_RANGE, kWidthRule);
     rc = validate_gates(gates, count, st->qubits);
     if (rc) return rc;
     std::lock_guard<std::recursive_mutex> lock(st->ctx->mu);

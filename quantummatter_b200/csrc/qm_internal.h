@@ -112,10 +112,32 @@ struct FusedPass {                  // 116 bytes
 inline int stage_lane_count(uint32_t reserved) { return (int)(reserved & 15u); }
 inline int stage_lane(uint32_t reserved, int i) { return (int)((reserved >> (4 + 4 * i)) & 15u); }
 
+// ---------------------------------------------------------------- dense fused gates
+// Fusion widths 2..6: the circuit becomes a sequence of fused gates, each a dense 2^m x 2^m
+// unitary on m <= width qubits applied as one sweep of the state (qm_dense.cpp, qm_dense.cu);
+// gates wider than the width run alone on the per-gate kernel.
+constexpr int kDenseMaxQubits = 6;
+struct DenseOp {
+    int32_t m;                      // qubits of the fused gate; 0: `gate` runs on the per-gate kernel
+    int32_t q[kDenseMaxQubits];     // its qubits, ascending (local bit i is qubit q[i])
+    int32_t gates;                  // circuit gates fused into it
+    int64_t matrix;                 // first complex element of its transposed unitary in dense_matrices
+    int64_t tc_image;               // first float of its tensor-core operand image in dense_tc, or -1
+    DevGate gate;
+};
+// Tile geometry of one dense fused gate (states of at least 9 qubits).
+struct DenseGeometry {
+    uint32_t qmask, lmask, copy_mask, outer_mask;
+    int32_t l_bits[12];
+    int32_t cols_bits, run_bits, copies, stride, buf_elems, nbuf, buf_offset;
+    size_t smem;
+    uint64_t items;
+};
+
 struct Plan {
     int32_t qubits = 0;
     int32_t precision = QM_FP64;
-    int32_t width = 0;              // 1: per-gate path
+    int32_t width = 0;              // 1: per-gate path; 2..6: dense fused gates
     std::vector<DevGate> gates;     // per-gate path
     std::vector<FusedPass> passes;  // fused path
     std::vector<FusedOp> ops;
@@ -135,6 +157,12 @@ struct Plan {
     bool start_zero = false;
     bool zero_fused = false;
     bool borrowed = false;          // d_ops belongs to a context buffer
+    std::vector<DenseOp> dense;         // dense fused gates (widths 2..6)
+    std::vector<double> dense_matrices; // their transposed unitaries, (re, im) pairs
+    double* d_dense = nullptr;          // device copy of dense_matrices
+    std::vector<float> dense_tc;        // tensor-core operand images of 6-qubit complex64 fused gates
+    float* d_dense_tc = nullptr;
+    int32_t* d_status = nullptr;        // status word the dense kernels set when a wait runs out
     int64_t planned_bytes = 0;
     int32_t launches = 0;
 };
@@ -150,6 +178,20 @@ void plan_release(Plan& plan);
 bool plan_fused(const std::vector<qm_gate>& gates, int qubits, int precision, int width, Plan& plan,
                 std::string& error, const std::vector<int32_t>* slots = nullptr);
 int default_block_qubits(int qubits, int precision);
+// Dense fused gates of at most `width` (1..6) qubits (qm_dense.cpp).
+bool plan_dense(const std::vector<qm_gate>& gates, int qubits, int precision, int width, Plan& plan,
+                std::string& error);
+bool dense_geometry(int qubits, int precision, const DenseOp& op, DenseGeometry& g);
+// One dense fused gate on a state (qm_dense.cu); `matrix` is its transposed unitary in device memory.
+cudaError_t launch_dense(void* amps, int qubits, int precision, const DenseOp& op, const double2* matrix,
+                         int32_t* status, int sm_count, cudaStream_t s);
+// 6-qubit fused gates on complex64 states of at least 11 qubits run on the tensor cores
+// (qm_dense_tc.cu, 3xTF32); QM_DENSE_TC=0 keeps them on the FP32 pipes.
+bool dense_tc_enabled();
+bool dense_tc_supported(int qubits, int precision, const DenseOp& op);
+void dense_tc_image(const double* transposed_unitary, std::vector<float>& image);
+cudaError_t launch_dense_tc(void* amps, int qubits, const DenseOp& op, const float* a_image, int32_t* status,
+                            int sm_count, cudaStream_t s);
 
 // ---------------------------------------------------------------- launchers (qm_kernels.cu)
 cudaError_t launch_gate(void* amps, int qubits, int precision, const DevGate& g, cudaStream_t s);
@@ -215,8 +257,11 @@ cudaError_t launch_expectation(const void* amps, int qubits, int precision, cons
 cudaError_t launch_finish_sums(const double* partials, int blocks, int columns, double* out,
                                cudaStream_t s);
 // One group of at most 8 terms sharing a flip mask into the [blocks][columns] partial table,
-// blocks = expectation_blocks(qubits) (at most 592).
+// blocks = expectation_blocks(qubits), never more than kReduceBlocksMax.
 constexpr int kPauliGroupMax = 8;
+// Grid cap of the reduction kernels (partial rows of masses, expectations, pattern masses): four
+// blocks per SM of a 148-SM B200.  Fixed-size scratch (qm_noalloc.cu) is sized from it.
+constexpr int kReduceBlocksMax = 148 * 4;
 int expectation_blocks(int qubits);
 cudaError_t launch_pauli_group(const void* amps, int qubits, int precision, uint32_t flip, int terms,
                                const uint32_t* sign, const int32_t* phase, const int32_t* column, int with_mass,

@@ -128,6 +128,17 @@ bool plan_fused_with(const std::vector<qm_gate>& gates, int qubits, int precisio
     const int64_t elem = precision == QM_FP32 ? 8 : 16;
     const int64_t n = int64_t(1) << qubits;
 
+    if (width >= 2 && width <= 8) {
+        if (slots) {
+            error = "batched plans need a fused block of at least 9 qubits";
+            return false;
+        }
+        if (width > kDenseMaxQubits) {
+            error = "fusion width must be 0, 1, 2..6 (dense fused gates) or 9..14 (fused blocks)";
+            return false;
+        }
+        return plan_dense(gates, qubits, precision, width, plan, error);
+    }
     const int kmax = precision == QM_FP32 ? 13 : 12;
     int k = width <= 0 ? default_block_qubits(qubits, precision) : std::min(width, kmax);
     k = std::min(k, qubits);
