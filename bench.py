@@ -134,8 +134,13 @@ def barrier_max(dist, value: float, local: int) -> float:
     return float(t.item())
 
 
+def first_layer_gates(qubits: int) -> int:
+    """Gates of the brick circuit's first layer: a U3 on every qubit, then CNOTs on the even pairs."""
+    return qubits + qubits // 2
+
+
 def cpu_baseline(circuit, qubits: int, sample_gates: int) -> dict:
-    """The reference's parallel/AVX-512 CPU path (oracle port) on the first gates of the workload."""
+    """The reference's parallel/AVX-512 CPU path (oracle port) on the first layer of the workload."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import numpy as np
 
@@ -152,8 +157,155 @@ def cpu_baseline(circuit, qubits: int, sample_gates: int) -> dict:
     orc.execute_parallel(sub, state, workers=threads)
     dt = time.perf_counter() - t0
     return {"value": sample_gates * (1 << qubits) / dt, "unit": "amp-updates/s", "cores": threads, "kind": "port",
-            "sample": f"first {sample_gates} gates (U3 layer 0) of the {qubits}-qubit circuit, AVX-512 + gate "
-                      f"blocking, {threads} worker threads, {dt:.2f} s"}
+            "sample": f"first layer of the {qubits}-qubit circuit ({sample_gates} gates: {qubits} U3 + "
+                      f"{sample_gates - qubits} CNOT) on the full state, AVX-512 + gate blocking, {threads} worker "
+                      f"threads, {dt:.2f} s"}
+
+
+class _DeviceBuffer:
+    """A raw device allocation of the library exposed through __cuda_array_interface__."""
+
+    def __init__(self, pointer: int, length: int, typestr: str):
+        self.__cuda_array_interface__ = {"shape": (length,), "typestr": typestr, "data": (pointer, False),
+                                         "version": 3, "strides": None}
+
+
+def max_abs_diff(a, b, chunk: int = 1 << 27) -> float:
+    """Largest complex |a_i - b_i| between two library states of one size, on the device (torch
+    views of the library's buffers, no copy), accumulated in FP64."""
+    import torch
+
+    from quantummatter_b200.backend import FP64
+    views = []
+    for st in (a, b):
+        typestr = "<f8" if st.precision == FP64 else "<f4"
+        views.append(torch.as_tensor(_DeviceBuffer(st.device_pointer(), 2 << st.QubitCount, typestr), device="cuda"))
+    worst = 0.0
+    for start in range(0, views[0].numel(), 2 * chunk):
+        x = views[0][start:start + 2 * chunk].double().view(-1, 2)
+        y = views[1][start:start + 2 * chunk].double().view(-1, 2)
+        worst = max(worst, torch.linalg.vector_norm(x - y, dim=1).max().item())
+    torch.cuda.synchronize()
+    return worst
+
+
+def fp32_side_run(ctx, circuit, state64, plan64, steps: int) -> dict:
+    """The complex64 form of the same circuit: its own plan timed on the device, and the largest
+    amplitude error of one evolution from |0...0> against the complex128 plan's."""
+    from quantummatter_b200.backend import FP32, DeviceState, Plan
+    qubits, gates = circuit.QubitCount, len(circuit.Operations)
+    plan32 = Plan(ctx, circuit, FP32)
+    try:
+        with DeviceState(ctx, qubits, FP32) as st:
+            plan32.execute(st)
+            seconds = [plan32.execute(st, profile=True).DeviceEvolutionSeconds for _ in range(steps)]
+            st.Reset()
+            plan32.execute(st)
+            state64.Reset()
+            plan64.execute(state64)
+            err = max_abs_diff(state64, st)
+        passes = plan32.stats()[0]
+    finally:
+        plan32.Dispose()
+    per = sum(seconds) / len(seconds)
+    return {"value": gates * (1 << qubits) / per, "unit": "amp-updates/s", "ms_per_step": 1e3 * per,
+            "steps": steps, "passes": passes, "max_abs_err_vs_fp64": err,
+            "err_reference": "complex128 compiled plan on the same GPU, one evolution from |0...0>"}
+
+
+def vqe_side_run(ctx, qubits: int = 22, vectors: int = 16) -> dict:
+    """A bounded batched-variational run beside the headline: the hardware-efficient ansatz (4
+    layers) on a `qubits`-site XXZ chain, `vectors` parameter vectors with full parameter-shift
+    gradients, FP32 and FP64 batched, against the plain form (one FP64 circuit at a time on a
+    resident state); warm-up with the full batch so no compilation or graph capture is timed."""
+    import numpy as np
+
+    from quantummatter_b200.backend import FP32, FP64, DeviceState
+    from quantummatter_b200.variational import B200VariationalEnergyEvaluator
+    from quantummatter_b200.workloads import hardware_efficient_ansatz, uniform_parameters, xxz_chain
+    c = hardware_efficient_ansatz(qubits, 4)
+    h = xxz_chain(qubits)
+    params = uniform_parameters(c.ParameterCount, vectors, -np.pi, np.pi, seed=qubits)
+    out, res = {}, {}
+    for name, prec in (("fp32", FP32), ("fp64", FP64)):
+        ev = B200VariationalEnergyEvaluator(ctx, prec)
+        ev.EvaluateBatch(c, h, params, withGradient=True)
+        t0 = time.perf_counter()
+        r = ev.EvaluateBatch(c, h, params, withGradient=True)
+        dt = time.perf_counter() - t0
+        res[name] = r
+        out[f"batched_{name}_evals_per_s"] = r.Circuits / dt
+    bound = [c.Bind(list(params[0]))] + [c.BindWithRotationShift(list(params[0]), r, s)
+                                         for r in range(8) for s in (np.pi / 2, -np.pi / 2)]
+    with DeviceState(ctx, qubits, FP64) as st:
+        st.Evolve(bound[0])
+        st.ExpectationEnergy(h)
+        t0 = time.perf_counter()
+        for b in bound:
+            st.Reset()
+            st.Evolve(b)
+            st.ExpectationEnergy(h)
+        plain = len(bound) / (time.perf_counter() - t0)
+    out["plain_fp64_evals_per_s"] = plain
+    out["batched_fp32_over_plain"] = out["batched_fp32_evals_per_s"] / plain
+    out["fp32_max_abs_dE_vs_fp64"] = float(np.max(np.abs(res["fp32"].Energies - res["fp64"].Energies)))
+    out["fp32_max_abs_dgrad_vs_fp64"] = float(np.max(np.abs(res["fp32"].Gradients - res["fp64"].Gradients)))
+    out["config"] = (f"hardware-efficient ansatz, 4 layers, {qubits}-site XXZ chain, {vectors} vectors with full "
+                     f"parameter-shift gradients ({res['fp64'].Circuits} circuits per batch)")
+    return out
+
+
+def run_widths(args) -> None:
+    """Fusion-width sweep of the 30-qubit brick (depth 40): widths k = 1..6 (dense fused gates of at
+    most k qubits, one sweep of the state each; k = 1 is one launch per gate) and the default fused
+    blocks of 12 qubits, in complex128 and complex64.  Per width and precision: amp-updates/s, the
+    plan's HBM GB/s (read + write of every sweep) against the copy peak, and the largest amplitude
+    error of one evolution from |0...0> against the complex128 fused-block plan, which equals the
+    per-gate path over all 2^30 amplitudes to 1e-12 (tests/test_headline_parity.py)."""
+    from quantummatter_b200.backend import FP32, FP64, B200BackendOptions, B200Context, DeviceState, Plan
+    from quantummatter_b200.workloads import brick_circuit
+    qubits, depth = args.qubits, args.depth
+    circuit = brick_circuit(qubits, depth)
+    gates, amps = len(circuit.Operations), 1 << qubits
+    peaks, peak_kind = measured_peaks()
+    hbm_peak = float(peaks.get("hbm_gbs", FALLBACK_HBM_GBS))
+    ctx = B200Context(B200BackendOptions(DeviceMemoryBudgetBytes=150 << 30, StagingMemoryBudgetBytes=1 << 30,
+                                         EnableProfiling=True))
+    widths = [int(w) for w in args.widths.split(",")]
+    rows = []
+    ref_plan = Plan(ctx, circuit, FP64)
+    ref = DeviceState(ctx, qubits, FP64)
+    ref_plan.execute(ref)
+    with ClockSampler(0) as clocks:
+        for precision, name in ((FP64, "fp64"), (FP32, "fp32")):
+            for width in widths:
+                plan = Plan(ctx, circuit, precision, width)
+                passes, launches, planned = plan.stats()
+                try:
+                    with DeviceState(ctx, qubits, precision) as st:
+                        plan.execute(st)
+                        err = max_abs_diff(ref, st)
+                        secs = [plan.execute(st, profile=True).DeviceEvolutionSeconds for _ in range(args.steps)]
+                finally:
+                    plan.Dispose()
+                per = sum(secs) / len(secs)
+                gbs = planned / per / 1e9
+                rows.append({"precision": name, "width": width,
+                             "scheme": "one launch per gate" if width == 1 else
+                             (f"dense fused gates of <= {width} qubits" if width <= 6 else f"fused blocks of {width} qubits"),
+                             "launches": launches, "amp_updates_per_s": gates * amps / per, "ms_per_step": 1e3 * per,
+                             "hbm_gbs": gbs, "hbm_frac": gbs / hbm_peak, "max_abs_err_vs_fp64": err})
+                print(json.dumps(rows[-1]), file=sys.stderr, flush=True)
+    ref.Dispose()
+    ref_plan.Dispose()
+    line = {"metric": f"amp-updates/s at {qubits}q by fusion width", "unit": "amp-updates/s",
+            "higher_is_better": True, "n_gpus": 1, "steps": args.steps, "data": "synthetic",
+            "config": {"workload": f"brick circuit, {qubits} qubits, depth {depth}, U3 + CNOT, {gates} gates",
+                       "peak_gbs": hbm_peak, "peak_source": peak_kind,
+                       "error_reference": "complex128 fused-block plan, one evolution from |0...0>"},
+            "sweep": rows, "clocks": clocks.summary()}
+    print(json.dumps(line), flush=True)
+    ctx.Dispose()
 
 
 def run_reference(args) -> None:
@@ -169,7 +321,7 @@ def run_reference(args) -> None:
     import oracle as orc
     from quantummatter_b200.circuit import QuantumCircuit
     circuit = brick_circuit(QUBITS, DEPTH)
-    sample = 4
+    sample = first_layer_gates(QUBITS)
     sub = QuantumCircuit(QUBITS)
     for op in circuit.Operations[:sample]:
         sub.AppendValidated(op)
@@ -189,9 +341,11 @@ def run_reference(args) -> None:
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": "brick circuit, 30 qubits, depth 40, U3 + CNOT, 1780 gates, complex128 state",
                    "qubits": QUBITS, "depth": DEPTH, "gates": len(circuit.Operations),
-                   "sample_per_step": f"first {sample} gates of the circuit on the full 2^30 state"},
+                   "sample_per_step": f"first layer of the circuit ({sample} gates: {QUBITS} U3 + "
+                                      f"{sample - QUBITS} CNOT) on the full 2^30 state"},
         "cpu_baseline": {"value": value, "unit": "amp-updates/s", "cores": threads, "kind": "port",
-                         "sample": f"first {sample} gates per step, {threads} threads, AVX-512 + gate blocking"},
+                         "sample": f"first layer ({sample} gates) per step, {threads} threads, AVX-512 + gate "
+                                   f"blocking"},
         "e2e": {"value": value, "unit": "amp-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -498,7 +652,10 @@ def main() -> None:
     ap.add_argument("--depth", type=int, default=DEPTH)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="brick", choices=["brick", "vqe", "trajectories", "serving"])
+    ap.add_argument("--no-side-runs", action="store_true",
+                    help="skip the complex64 and batched-variational side runs of the default line")
+    ap.add_argument("--workload", default="brick", choices=["brick", "vqe", "trajectories", "serving", "widths"])
+    ap.add_argument("--widths", default="1,2,3,4,5,6,12", help="widths workload: fusion widths to sweep")
     ap.add_argument("--circuit", default="brick", choices=["brick", "qft", "grover"],
                     help="brick workload: the circuit (qft and grover: the algorithm builders at --qubits)")
     ap.add_argument("--sizes", default="16,18,20,22", help="vqe workload: qubit counts")
@@ -524,6 +681,9 @@ def main() -> None:
         return
     if args.workload == "serving":
         run_serving(args)
+        return
+    if args.workload == "widths":
+        run_widths(args)
         return
 
     dist, rank, world, local = dist_setup(args.gpus)
@@ -551,7 +711,7 @@ def main() -> None:
         described = f"brick circuit, {qubits} qubits, depth {depth}, U3 + CNOT"
     gates = len(circuit.Operations)
     amps = 1 << qubits
-    ctx = B200Context(B200BackendOptions(DeviceIndex=local, DeviceMemoryBudgetBytes=80 << 30,
+    ctx = B200Context(B200BackendOptions(DeviceIndex=local, DeviceMemoryBudgetBytes=150 << 30,
                                          StagingMemoryBudgetBytes=80 << 30, EnableProfiling=True,
                                          FusionWidth=args.width))
     plan = Plan(ctx, circuit, precision, args.width)
@@ -613,10 +773,14 @@ def main() -> None:
         backend.Dispose()
 
     fp64 = fp64_roofline(fp64_flops, args.steps, total, launches, clocks.summary())
+    side32 = side_vqe = None
+    if rank == 0 and world == 1 and precision == FP64 and args.circuit == "brick" and not args.no_side_runs:
+        side32 = fp32_side_run(ctx, circuit, state, plan, steps=3)
+        side_vqe = vqe_side_run(ctx)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         state.Dispose()
-        cpu = cpu_baseline(circuit, qubits, 8)
+        cpu = cpu_baseline(circuit, qubits, first_layer_gates(qubits) if args.circuit == "brick" else 8)
 
     if rank == 0:
         line = {
@@ -645,6 +809,10 @@ def main() -> None:
             line["e2e"] = e2e
         if cpu:
             line["cpu_baseline"] = cpu
+        if side32:
+            line["fp32"] = side32
+        if side_vqe:
+            line["vqe_22q"] = side_vqe
         print(json.dumps(line), flush=True)
     plan.Dispose()
     try:

@@ -102,7 +102,10 @@ typedef struct qm_options {
     int32_t enable_profiling;       /* fills qm_profile in the *_profiled calls */
     int64_t device_budget_bytes;    /* maximum bytes of device states held by the context */
     int64_t staging_budget_bytes;   /* maximum pinned host staging bytes */
-    int32_t fusion_width;           /* 0 = planner default; 1 = one launch per gate; else block qubits */
+    int32_t fusion_width;           /* 0 = planner default (fused blocks of 12 qubits); 1 = one launch
+                                       per gate; 2..6 = dense fused gates of at most that many qubits,
+                                       one sweep of the state each; 9..14 = fused blocks of that many
+                                       qubits.  7 and 8 give QM_E_RANGE. */
     int32_t reserved[7];
 } qm_options;
 
@@ -203,6 +206,28 @@ int32_t qm_plan_execute(qm_plan* plan, qm_state* state, qm_profile* profile);
 /* passes, kernel launches and planned DRAM bytes of one execution. */
 int32_t qm_plan_stats(const qm_plan* plan, int32_t* passes, int32_t* launches, int64_t* planned_bytes);
 int32_t qm_plan_destroy(qm_plan* plan);
+
+/* The engine's autotuner: plans the gates at each candidate fusion width, times one execution of
+ * each on a scratch state of that size (after an untimed one that compiles its kernels; the
+ * scratch is freed before returning), and returns the plan of the fastest, as qm_plan_create does,
+ * with its width in *chosen (may be NULL).  The choice is cached for the process per qubit count,
+ * precision and gate structure (kernels, targets, controls; not coefficients), so circuits that
+ * differ only in angles are timed once.  candidates NULL / candidate_count 0: fused blocks of 10,
+ * 11 and 12 qubits, plus 13 and dense fused gates of 5 and 6 qubits for QM_FP32.  Additive. */
+int32_t qm_plan_autotune(qm_context* context, int32_t qubits, int32_t precision, const qm_gate* gates,
+                         int32_t count, const int32_t* candidates, int32_t candidate_count, qm_plan** plan,
+                         int32_t* chosen);
+
+/* One execution of a plan on a state captured as a CUDA graph: every pass (or fused gate) of the
+ * plan becomes a node, and a launch replays them with one submission on the context's stream.
+ * The plan and the state must outlive the graph; a launch evolves the state it was captured on,
+ * in place, exactly as qm_plan_execute does (the capture itself runs nothing).  Execute the plan
+ * once before capturing it, so that its kernels are loaded.  Additive (the reference launches one
+ * kernel per gate and synchronises every 32, CudaStateVectorBackend.cs:155-159). */
+typedef struct qm_graph qm_graph;
+int32_t qm_graph_create(qm_plan* plan, qm_state* state, qm_graph** graph);
+int32_t qm_graph_launch(qm_graph* graph, qm_profile* profile);
+int32_t qm_graph_destroy(qm_graph* graph);
 
 /* Host-only inspection of the fused schedule the planner builds for a gate list (no
  * device needed): pass headers and the op program each pass's kernel interprets.

@@ -131,6 +131,10 @@ SIGNATURES = {
     "qm_plan_execute": (I32, [P, P, C.POINTER(Profile)]),
     "qm_plan_stats": (I32, [P, I32P, I32P, I64P]),
     "qm_plan_destroy": (I32, [P]),
+    "qm_plan_autotune": (I32, [P, I32, I32, P, I32, I32P, I32, C.POINTER(P), I32P]),
+    "qm_graph_create": (I32, [P, P, C.POINTER(P)]),
+    "qm_graph_launch": (I32, [P, C.POINTER(Profile)]),
+    "qm_graph_destroy": (I32, [P]),
     "qm_plan_program": (I32, [I32, I32, C.POINTER(Gate), I32, I32, I32P, C.POINTER(FusedPassInfo), I32, I32P,
                               C.POINTER(FusedOpInfo), I32, I64P]),
     "qm_qubit_masses": (I32, [P, I32, DP, DP]),

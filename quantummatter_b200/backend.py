@@ -270,6 +270,22 @@ class Plan:
         self.qubits = circuit.QubitCount
         self.precision = precision
 
+    @classmethod
+    def autotune(cls, context: B200Context, circuit: QuantumCircuit, precision: int = FP64,
+                 candidates: Sequence[int] | None = None) -> "Plan":
+        """The plan of the fastest candidate fusion width, timed on the device (qm_plan_autotune);
+        `width` holds the choice, cached per gate structure for the process."""
+        gates, n = prepare(circuit)
+        h, chosen = C.c_void_p(), C.c_int32()
+        cand = list(candidates or [])
+        arr = (C.c_int32 * len(cand))(*cand) if cand else None
+        check(load().qm_plan_autotune(context.handle, circuit.QubitCount, precision, gates, n, arr, len(cand),
+                                      C.byref(h), C.byref(chosen)))
+        plan = cls.__new__(cls)
+        plan._h, plan.context, plan.qubits, plan.precision = h, context, circuit.QubitCount, precision
+        plan.width = chosen.value
+        return plan
+
     def stats(self) -> tuple[int, int, int]:
         passes, launches, bytes_ = C.c_int32(), C.c_int32(), C.c_int64()
         check(load().qm_plan_stats(self._h, C.byref(passes), C.byref(launches), C.byref(bytes_)))
@@ -280,9 +296,39 @@ class Plan:
         check(load().qm_plan_execute(self._h, state.handle, C.byref(prof) if prof is not None else None))
         return _profile(prof) if prof is not None else None
 
+    def capture(self, state: "DeviceState") -> "CapturedExecution":
+        """One execution of this plan on `state` as a CUDA graph (qm_graph_create)."""
+        return CapturedExecution(self, state)
+
     def Dispose(self) -> None:
         if self._h is not None:
             load().qm_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.Dispose()
+        except Exception:
+            pass
+
+
+class CapturedExecution:
+    """A plan's execution on one state captured as a CUDA graph; launch() replays it in place."""
+
+    def __init__(self, plan: Plan, state: "DeviceState"):
+        h = C.c_void_p()
+        check(load().qm_graph_create(plan._h, state.handle, C.byref(h)))
+        self._h = h
+        self.plan, self.state = plan, state
+
+    def launch(self, profile: bool = False) -> B200ExecutionProfile | None:
+        prof = _lib.Profile() if profile else None
+        check(load().qm_graph_launch(self._h, C.byref(prof) if prof is not None else None))
+        return _profile(prof) if prof is not None else None
+
+    def Dispose(self) -> None:
+        if self._h is not None:
+            load().qm_graph_destroy(self._h)
             self._h = None
 
     def __del__(self):

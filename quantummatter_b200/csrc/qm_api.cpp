@@ -10,7 +10,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -536,21 +538,22 @@ extern "C" int32_t qm_execute_host(qm_context* ctx, int32_t qubits, const qm_ope
     if (rc) return rc;
     std::vector<qm_gate> gates((size_t)count);
     for (int32_t i = 0; i < count; ++i) prepare_one(ops[i], gates[(size_t)i]);
-    Plan plan;
-    rc = build_plan(ctx, qubits, QM_FP64, gates.data(), count, 0, plan, true);
-    if (rc) { free_plan(plan); return rc; }
     void* dev = nullptr;
     rc = device_buffer(ctx, (size_t)bytes, &dev);
-    if (rc) { free_plan(plan); return rc; }
+    if (rc) return rc;
 
     cudaEvent_t t0 = nullptr, t1 = nullptr, t2 = nullptr, t3 = nullptr;
     if (profile) {
         cudaEventCreate(&t0); cudaEventCreate(&t1); cudaEventCreate(&t2); cudaEventCreate(&t3);
         cudaEventRecord(t0, ctx->stream);
     }
+    // The upload is queued first: from a page-locked buffer it returns at once, and the plan is
+    // built (and its compiled passes looked up) on the host while the copy engine moves the state.
     cudaError_t e = host_to_device(ctx, dev, amps, (size_t)bytes);
     if (e == cudaSuccess && profile) cudaEventRecord(t1, ctx->stream);
-    if (e == cudaSuccess) rc = run_plan(ctx, plan, dev, cancel);
+    Plan plan;
+    if (e == cudaSuccess) rc = build_plan(ctx, qubits, QM_FP64, gates.data(), count, 0, plan, true);
+    if (e == cudaSuccess && rc == QM_OK) rc = run_plan(ctx, plan, dev, cancel);
     if (e == cudaSuccess && rc == QM_OK) {
         if (profile) cudaEventRecord(t2, ctx->stream);
         e = cudaStreamSynchronize(ctx->stream);
@@ -909,6 +912,187 @@ extern "C" int32_t qm_plan_execute(qm_plan* p, qm_state* st, qm_profile* profile
         return fail(QM_E_ARG, "plan and state sizes must match");
     std::lock_guard<std::recursive_mutex> lock(st->ctx->mu);
     return execute_plan(st, p->plan, profile);
+}
+
+// ====================================================================== autotuning
+
+namespace {
+
+// Fusion widths chosen by qm_plan_autotune, per (qubits, precision, gate structure): the
+// structure is every gate's kernel, target, controls and swap operand, not its coefficients, so
+// circuits that differ only in angles share a choice.
+std::mutex g_tune_mutex;
+std::map<std::vector<int64_t>, int32_t> g_tune_cache;
+
+std::vector<int64_t> structure_key(int32_t qubits, int32_t precision, const qm_gate* gates, int32_t count) {
+    std::vector<int64_t> key;
+    key.reserve(2 + (size_t)count);
+    key.push_back(qubits);
+    key.push_back(precision);
+    for (int32_t i = 0; i < count; ++i) {
+        const qm_gate& g = gates[i];
+        key.push_back(((int64_t)g.kernel << 56) | ((int64_t)(g.target & 0xff) << 48) |
+                      ((int64_t)((g.swap_control + 1) & 0xff) << 40) | (int64_t)g.control_mask);
+    }
+    return key;
+}
+
+}  // namespace
+
+extern "C" int32_t qm_plan_autotune(qm_context* ctx, int32_t qubits, int32_t precision, const qm_gate* gates,
+                                    int32_t count, const int32_t* candidates, int32_t candidate_count, qm_plan** out,
+                                    int32_t* chosen) {
+    if (!ctx || !out) return fail(QM_E_ARG, "null argument");
+    *out = nullptr;
+    if (qubits < 1 || qubits > 30) return fail(QM_E_RANGE, "qubits must be between 1 and 30");
+    if (precision != QM_FP64 && precision != QM_FP32) return fail(QM_E_RANGE, "unknown precision");
+    if (candidate_count < 0 || (candidate_count > 0 && !candidates)) return fail(QM_E_ARG, "candidates");
+    int32_t rc = validate_gates(gates, count, qubits);
+    if (rc) return rc;
+    std::vector<int32_t> widths(candidates, candidates + candidate_count);
+    if (widths.empty()) {
+        widths = {10, 11, 12};
+        if (precision == QM_FP32) widths.insert(widths.end(), {13, 5, 6});
+    }
+    for (int32_t w : widths)
+        if (w == 0 || !valid_width(w)) return fail(QM_E_RANGE, kWidthRule);
+    const std::vector<int64_t> key = structure_key(qubits, precision, gates, count);
+    int32_t best = 0;
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) best = it->second;
+    }
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    if (ctx->disposed) return fail(QM_E_DISPOSED, "context disposed");
+    QM_CUDA(cudaSetDevice(ctx->device));
+    if (best == 0 && widths.size() == 1) best = widths[0];
+    if (best == 0) {
+        // time one execution of each candidate (after one untimed, which compiles and loads its
+        // kernels) on a scratch state; the scratch is freed before the chosen plan is built
+        const size_t bytes = (size_t)(precision == QM_FP32 ? 8 : 16) << qubits;
+        if ((int64_t)bytes + ctx->device_in_use > ctx->device_budget)
+            return fail(QM_E_BUDGET, "autotuning needs a scratch state within the device budget");
+        void* scratch = nullptr;
+        QM_CUDA(cudaMalloc(&scratch, bytes));
+        double best_s = 0;
+        for (int32_t w : widths) {
+            Plan plan;
+            rc = build_plan(ctx, qubits, precision, gates, count, w, plan);
+            if (rc == QM_OK) {
+                jit_prepare(plan);
+                launch_reset(scratch, qubits, precision, ctx->stream);
+                rc = run_plan(ctx, plan, scratch, nullptr);
+            }
+            if (rc == QM_OK) {
+                cudaEventRecord(ctx->ev_start, ctx->stream);
+                rc = run_plan(ctx, plan, scratch, nullptr);
+                cudaEventRecord(ctx->ev_stop, ctx->stream);
+            }
+            const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+            if (rc == QM_OK && e == cudaSuccess) rc = dense_status(plan);
+            free_plan(plan);
+            if (e != cudaSuccess) {
+                cudaFree(scratch);
+                return cuda_fail(e, "qm_plan_autotune");
+            }
+            if (rc) continue;  // a candidate this circuit cannot use (e.g. a batch-only width)
+            const double sec = seconds_between(ctx->ev_start, ctx->ev_stop);
+            if (best == 0 || sec < best_s) {
+                best = w;
+                best_s = sec;
+            }
+        }
+        cudaFree(scratch);
+        if (best == 0) return fail(QM_E_ARG, "no candidate fusion width plans this circuit");
+        std::lock_guard<std::mutex> tl(g_tune_mutex);
+        g_tune_cache[key] = best;
+    }
+    rc = qm_plan_create(ctx, qubits, precision, gates, count, best, out);
+    if (rc == QM_OK && chosen) *chosen = best;
+    return rc;
+}
+
+// ====================================================================== captured executions
+
+struct qm_graph {
+    qm_context* ctx = nullptr;
+    qm_plan* plan = nullptr;
+    qm_state* state = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+extern "C" int32_t qm_graph_create(qm_plan* p, qm_state* st, qm_graph** out) {
+    if (!p || !st || !out) return fail(QM_E_ARG, "null argument");
+    *out = nullptr;
+    if (p->ctx != st->ctx) return fail(QM_E_ARG, "plan and state belong to different contexts");
+    if (p->plan.qubits != st->qubits || p->plan.precision != st->precision)
+        return fail(QM_E_ARG, "plan and state sizes must match");
+    qm_context* ctx = st->ctx;
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    if (ctx->disposed) return fail(QM_E_DISPOSED, "context disposed");
+    QM_CUDA(cudaSetDevice(ctx->device));
+    // The capture records the plan's launches only (nothing runs); kernel attributes and compiled
+    // passes are set up by the plan's first execution, which the caller makes before capturing.
+    QM_CUDA(cudaStreamSynchronize(ctx->stream));
+    std::unique_ptr<qm_graph> g(new qm_graph());
+    g->ctx = ctx;
+    g->plan = p;
+    g->state = st;
+    QM_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+    int32_t rc = run_plan(ctx, p->plan, st->amps, nullptr);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+    if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    g->graph = graph;
+    const cudaError_t ie = cudaGraphInstantiate(&g->exec, graph, 0);
+    if (ie != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        return cuda_fail(ie, "cudaGraphInstantiate");
+    }
+    *out = g.release();
+    return QM_OK;
+}
+
+extern "C" int32_t qm_graph_launch(qm_graph* g, qm_profile* profile) {
+    if (!g) return fail(QM_E_ARG, "graph is null");
+    qm_context* ctx = g->ctx;
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    if (ctx->disposed) return fail(QM_E_DISPOSED, "context disposed");
+    QM_CUDA(cudaSetDevice(ctx->device));
+    if (profile) QM_CUDA(cudaEventRecord(ctx->ev_start, ctx->stream));
+    QM_CUDA(cudaGraphLaunch(g->exec, ctx->stream));
+    if (profile) QM_CUDA(cudaEventRecord(ctx->ev_stop, ctx->stream));
+    QM_CUDA(cudaStreamSynchronize(ctx->stream));
+    int32_t rc = dense_status(g->plan->plan);
+    if (rc) return rc;
+    if (profile) {
+        std::memset(profile, 0, sizeof *profile);
+        profile->device_seconds = seconds_between(ctx->ev_start, ctx->ev_stop);
+        profile->state_bytes = g->state->bytes;
+        profile->kernel_launches = g->plan->plan.launches;
+        profile->passes = (int32_t)g->plan->plan.passes.size();
+        profile->planned_bytes = g->plan->plan.planned_bytes;
+    }
+    return QM_OK;
+}
+
+extern "C" int32_t qm_graph_destroy(qm_graph* g) {
+    if (!g) return QM_OK;
+    if (g->ctx) {
+        std::lock_guard<std::recursive_mutex> lock(g->ctx->mu);
+        cudaSetDevice(g->ctx->device);
+        cudaStreamSynchronize(g->ctx->stream);
+    }
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
+    return QM_OK;
 }
 
 extern "C" int32_t qm_execute(qm_state* st, const qm_gate* gates, int32_t count, int32_t width, qm_profile* profile) {
