@@ -517,7 +517,7 @@ def run_trajectories(args) -> None:
         dist.destroy_process_group()
 
 
-def serving_requests(count: int, rate: float, precision: int, seed: int, sessions):
+def serving_requests(count: int, rate: float, precision: int, seed: int, sessions, kinds: int = 3):
     """Poisson arrivals at `rate`; each request an expectation of a random brick circuit (Z_i and
     Z_i Z_i+1), 1000 shots of one, or a VQE step of a random session (TFIM chain, hardware-efficient
     ansatz of 2 layers); qubits uniform in [10, 28], brick depth uniform in [10, 100]."""
@@ -531,7 +531,7 @@ def serving_requests(count: int, rate: float, precision: int, seed: int, session
     for i in range(count):
         t += rng.exponential(1.0 / rate)
         arrivals.append(t)
-        kind = int(rng.integers(3))
+        kind = int(rng.integers(kinds))
         if kind == 2:
             reqs.append(VqeStepRequest(sessions[int(rng.integers(len(sessions)))]))
             continue
@@ -578,6 +578,123 @@ def serving_summary(responses, reqs, makespan: float) -> dict:
             "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3),
             "mean_vqe_batch": float(np.mean([r.batch for r in responses if r.kind == "vqe_step"] or [1])),
             "per_kind": per_kind}
+
+
+def run_serving_closed(args) -> None:
+    """Closed-loop serving: one client thread per VQE session submits its next step only when the
+    previous one returned (16 sessions: TFIM chains of 14, 16, 18 and 20 sites, 4 each, 2-layer
+    hardware-efficient ansatz), beside `--background` clients that keep one expectation or
+    1000-shot request each in flight (random brick circuits of 10-28 qubits).  The server runs
+    at its own pace, so its throughput is capacity, not offered load.  The plain form runs the same
+    VQE steps one circuit at a time in FP64."""
+    import numpy as np
+
+    from quantummatter_b200.backend import FP32, FP64, B200BackendOptions, B200Context
+    from quantummatter_b200.serving import B200Server, VqeSession, VqeStepRequest, serve_plain
+    from quantummatter_b200.workloads import hardware_efficient_ansatz, tfim_chain
+    sizes = [int(x) for x in args.session_sizes.split(",")]
+    steps = args.session_steps
+
+    def sessions(prec):
+        rng = np.random.default_rng(17)
+        out = []
+        for n in sizes:
+            c = hardware_efficient_ansatz(n, 2)
+            for k in range(args.sessions_per_size):
+                out.append(VqeSession(c, tfim_chain(n, seed=100 * n + k), rng.uniform(-np.pi, np.pi, c.ParameterCount),
+                                      step_size=0.05, precision=prec))
+        return out
+
+    def evals(s):
+        return 1 + 2 * len(s.circuit.RotationParameterIndices)
+
+    results = {}
+    clocks = ClockSampler(0)
+    with clocks:
+        for name, prec in (("fp32", FP32), ("fp64", FP64)):
+            ss = sessions(prec)
+            background, _ = serving_requests(args.background * 40, 1.0, prec, seed=23, sessions=[], kinds=2)
+            with B200Server(workers=args.workers, budget_bytes=args.serve_budget << 30,
+                            context_budget_bytes=24 << 30, cache_bytes=8 << 30) as server:
+                warm = sessions(prec)  # plans and kernels of every size, outside the timed region
+                for f in [server.submit(VqeStepRequest(s)) for s in warm]:
+                    f.result()
+                for f in [server.submit(r) for r in background[:4]]:
+                    f.result()
+                responses, lock, stop = [], threading.Lock(), threading.Event()
+
+                def vqe_client(s):
+                    for _ in range(steps):
+                        r = server.submit(VqeStepRequest(s)).result()
+                        with lock:
+                            responses.append(r)
+
+                def background_client(k):
+                    i = k
+                    while not stop.is_set() and i < len(background):
+                        r = server.submit(background[i]).result()
+                        with lock:
+                            responses.append(r)
+                        i += args.background
+
+                t0 = time.perf_counter()
+                threads = [threading.Thread(target=vqe_client, args=(s,)) for s in ss]
+                bg = [threading.Thread(target=background_client, args=(k,)) for k in range(args.background)]
+                for t in threads + bg:
+                    t.start()
+                for t in threads:
+                    t.join()
+                makespan = time.perf_counter() - t0
+                stop.set()
+                for t in bg:
+                    t.join()
+                stats = server.stats()
+            vq = [r for r in responses if r.kind == "vqe_step"]
+            lat = np.array([r.latency for r in responses if r.finished - t0 <= makespan + 1e-9])
+            vlat = np.array([r.latency for r in vq])
+            results[name] = {"makespan_s": makespan, "vqe_steps": len(vq),
+                             "energy_evals_per_s": steps * sum(evals(s) for s in ss) / makespan,
+                             "requests_per_s": len(lat) / makespan,
+                             "mean_vqe_batch": float(np.mean([r.batch for r in vq])),
+                             "max_vqe_batch": int(max(r.batch for r in vq)),
+                             "vqe_p50_ms": float(np.percentile(vlat, 50) * 1e3),
+                             "vqe_p99_ms": float(np.percentile(vlat, 99) * 1e3),
+                             "all_p50_ms": float(np.percentile(lat, 50) * 1e3),
+                             "all_p99_ms": float(np.percentile(lat, 99) * 1e3),
+                             "background_requests": len(responses) - len(vq),
+                             "server": {k: stats[k] for k in ("jobs", "vqe_jobs", "vqe_steps", "max_batch",
+                                                              "peak_reserved_bytes", "budget_bytes")}}
+        # plain form: the same VQE steps, one circuit at a time, FP64, one request after another
+        ctx = B200Context(B200BackendOptions(DeviceMemoryBudgetBytes=24 << 30, StagingMemoryBudgetBytes=1 << 30))
+        ss = sessions(FP64)
+        serve_plain([VqeStepRequest(s) for s in sessions(FP64)[::args.sessions_per_size]], ctx)  # warm-up
+        sample = ss[::args.sessions_per_size]  # one session per size, every step
+        t0 = time.perf_counter()
+        plain = []
+        for _ in range(steps):
+            plain += serve_plain([VqeStepRequest(s) for s in sample], ctx)
+        plain_dt = time.perf_counter() - t0
+        ctx.Dispose()
+        plain_evals = steps * sum(evals(s) for s in sample) / plain_dt
+        plat = np.array([r.latency for r in plain])
+        results["plain_fp64"] = {"energy_evals_per_s": plain_evals, "seconds": plain_dt,
+                                 "vqe_p50_ms": float(np.percentile(plat, 50) * 1e3),
+                                 "vqe_p99_ms": float(np.percentile(plat, 99) * 1e3),
+                                 "sample": f"one session per size ({len(sample)}), {steps} steps each"}
+    line = {
+        "metric": "served energy evals/s (closed loop)", "value": results["fp32"]["energy_evals_per_s"],
+        "unit": "evals/s", "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"closed loop: {len(sizes) * args.sessions_per_size} VQE sessions (TFIM chains of "
+                               f"{sizes} sites, {args.sessions_per_size} each, 2-layer hardware-efficient ansatz), "
+                               f"{steps} steps each, one step in flight per session; {args.background} background "
+                               "clients with expectation / 1000-shot requests (brick circuits, 10-28 qubits)",
+                   "workers": args.workers, "budget_gib": args.serve_budget},
+        "p50_ms": results["fp32"]["vqe_p50_ms"], "p99_ms": results["fp32"]["vqe_p99_ms"],
+        "fp32_over_plain_fp64": results["fp32"]["energy_evals_per_s"] / plain_evals,
+        "fp64_over_plain_fp64": results["fp64"]["energy_evals_per_s"] / plain_evals,
+        "results": results, "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
 
 
 def run_serving(args) -> None:
@@ -669,6 +786,12 @@ def main() -> None:
     ap.add_argument("--sessions", type=int, default=12, help="serving workload: VQE sessions")
     ap.add_argument("--workers", type=int, default=4, help="serving workload: worker streams")
     ap.add_argument("--serve-budget", type=int, default=96, help="serving workload: admission budget, GiB")
+    ap.add_argument("--serve-mode", default="open", choices=["open", "closed"],
+                    help="serving workload: Poisson arrivals (open) or clients that wait for each result (closed)")
+    ap.add_argument("--session-sizes", default="14,16,18,20", help="closed serving: VQE session sizes")
+    ap.add_argument("--sessions-per-size", type=int, default=4, help="closed serving: sessions per size")
+    ap.add_argument("--session-steps", type=int, default=4, help="closed serving: steps per session")
+    ap.add_argument("--background", type=int, default=4, help="closed serving: expectation/shots clients")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -680,7 +803,7 @@ def main() -> None:
         run_trajectories(args)
         return
     if args.workload == "serving":
-        run_serving(args)
+        run_serving_closed(args) if args.serve_mode == "closed" else run_serving(args)
         return
     if args.workload == "widths":
         run_widths(args)

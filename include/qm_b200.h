@@ -409,6 +409,82 @@ int32_t qm_vqe_evaluate_coefficients(qm_context* context, int32_t qubits, int32_
                                      const double* parameters, int32_t vectors, int32_t with_gradient,
                                      double* energies, double* gradients, qm_vqe_stats* stats);
 
+/* ---------------------------------------------------------------- serving */
+
+/* A request server on one GPU; no reference counterpart (applications call the reference's port
+ * one circuit at a time: StateVector.Evolve + ExpectationValue, StateVector.Observations.cs:107-141;
+ * StateVectorSimulator.Run, StateVectorSimulator.cs:37-101; VariationalEnergyEvaluator.
+ * EvaluateWithGradient, VariationalEnergyEvaluator.cs:34-86).  Requests from any host thread are
+ * admitted by the bytes of their state (16 * 2^n complex128, 8 * 2^n complex64) against
+ * budget_bytes, oldest first (a younger request passes only while an older one does not fit); each
+ * of `workers` threads runs jobs on its own context and CUDA stream, so jobs overlap on the device.
+ * A VQE session keeps its parameters in the server; waiting steps of sessions that share an ansatz
+ * structure and Pauli strings run as one batch (qm_vqe_evaluate_coefficients), a session never has
+ * two steps in flight, and each step ends with p - step_size * gradient rounded once (VqeSolver.cs:76).
+ * Results equal those of the request run alone. */
+typedef struct qm_server qm_server;
+typedef struct qm_serve_options {
+    int32_t device_index;
+    int32_t workers;                /* worker threads, 1..64 */
+    int64_t budget_bytes;           /* admission budget over the requests in flight */
+    int64_t context_budget_bytes;   /* device budget of each worker's context */
+    int64_t cache_bytes;            /* device states each worker keeps for reuse */
+    int32_t max_batch;              /* VQE steps per device batch (0: 64) */
+    int32_t reserved[5];
+} qm_serve_options;
+
+enum { QM_SERVE_EXPECTATION = 0, QM_SERVE_SHOTS = 1, QM_SERVE_VQE_STEP = 2 };
+
+typedef struct qm_serve_result {
+    int32_t kind;                   /* QM_SERVE_* */
+    int32_t status;                 /* QM_OK or the error of the request's execution (qm_last_error) */
+    int32_t batch;                  /* requests evaluated in the same device batch */
+    int32_t ambiguous;              /* shots drawn within the rounding margin of a CDF boundary */
+    int32_t values;                 /* doubles written to values: per-term <P_t> or the VQE gradient */
+    int32_t outcomes;               /* int64s written to outcomes: one basis index per shot */
+    int32_t parameters;             /* doubles written to parameters: the session's after the step */
+    int32_t reserved;
+    double mass;                    /* expectation: Born mass of the final state */
+    double energy;                  /* VQE step: the energy before the update */
+    double submitted, started, finished;  /* seconds since qm_serve_create */
+} qm_serve_result;
+
+typedef struct qm_serve_stats {
+    int64_t submitted, completed, jobs, vqe_jobs, vqe_steps;
+    int64_t budget_bytes, reserved_bytes, peak_reserved_bytes;
+    int32_t queued, running, max_batch, reserved;
+} qm_serve_stats;
+
+int32_t qm_serve_create(const qm_serve_options* options, qm_server** server);
+/* Waits for the jobs on the device, cancels waiting requests (QM_E_CANCELLED) and frees everything. */
+int32_t qm_serve_destroy(qm_server* server);
+/* <P_t> / <psi|psi> of every term on the circuit's final state from |0...0> (coefficients ignored). */
+int32_t qm_serve_submit_expectation(qm_server* server, int32_t qubits, int32_t precision,
+                                    const qm_operation* operations, int32_t count, const qm_pauli_term* terms,
+                                    int32_t term_count, int64_t* request);
+/* Terminal samples of the circuit's final state, one per draw in [0, 1) (qm_sample). */
+int32_t qm_serve_submit_shots(qm_server* server, int32_t qubits, int32_t precision, const qm_operation* operations,
+                              int32_t count, const double* draws, int32_t shots, int64_t* request);
+/* A VQE session: the ansatz template (qm_vqe_evaluate), the Hamiltonian with its coefficients,
+ * the initial parameters and the steepest-descent step size. */
+int32_t qm_serve_session_create(qm_server* server, int32_t qubits, int32_t precision,
+                                const qm_template_op* operations, int32_t operation_count, int32_t parameter_count,
+                                const qm_pauli_term* terms, int32_t term_count, const double* parameters,
+                                double step_size, int64_t* session);
+int32_t qm_serve_session_parameters(qm_server* server, int64_t session, double* parameters, int32_t count,
+                                    int64_t* steps);
+int32_t qm_serve_session_destroy(qm_server* server, int64_t session);  /* QM_E_ARG while steps are in flight */
+/* One energy + parameter-shift gradient at the session's parameters, then the update. */
+int32_t qm_serve_submit_vqe_step(qm_server* server, int64_t session, int64_t* request);
+/* Waits up to timeout_seconds (0: polls) for the request; *done = 1 once it finished. */
+int32_t qm_serve_wait(qm_server* server, int64_t request, double timeout_seconds, int32_t* done);
+/* Copies a finished request's result and outputs and forgets the request.  Buffers may be NULL when
+ * the request has no such output; QM_E_RANGE when one is too small (the request is kept). */
+int32_t qm_serve_take_result(qm_server* server, int64_t request, qm_serve_result* result, double* values,
+                             int32_t max_values, int64_t* outcomes, int32_t max_outcomes, double* parameters,
+                             int32_t max_parameters);
+int32_t qm_serve_get_stats(qm_server* server, qm_serve_stats* stats);
+
 /* ---------------------------------------------------------------- noise trajectories */
 
 /* One channel placement of a NoisyCircuit (src/QuantumMatter.Core/Noise/NoisyCircuit.cs:38-48):

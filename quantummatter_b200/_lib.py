@@ -89,6 +89,26 @@ class TrajectoryOutputs(C.Structure):
                 ("probability_means", C.POINTER(C.c_double)), ("probability_stderr", C.POINTER(C.c_double))]
 
 
+class ServeOptions(C.Structure):
+    _fields_ = [("device_index", C.c_int32), ("workers", C.c_int32), ("budget_bytes", C.c_int64),
+                ("context_budget_bytes", C.c_int64), ("cache_bytes", C.c_int64), ("max_batch", C.c_int32),
+                ("reserved", C.c_int32 * 5)]
+
+
+class ServeResult(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("status", C.c_int32), ("batch", C.c_int32), ("ambiguous", C.c_int32),
+                ("values", C.c_int32), ("outcomes", C.c_int32), ("parameters", C.c_int32), ("reserved", C.c_int32),
+                ("mass", C.c_double), ("energy", C.c_double), ("submitted", C.c_double), ("started", C.c_double),
+                ("finished", C.c_double)]
+
+
+class ServeStats(C.Structure):
+    _fields_ = [("submitted", C.c_int64), ("completed", C.c_int64), ("jobs", C.c_int64), ("vqe_jobs", C.c_int64),
+                ("vqe_steps", C.c_int64), ("budget_bytes", C.c_int64), ("reserved_bytes", C.c_int64),
+                ("peak_reserved_bytes", C.c_int64), ("queued", C.c_int32), ("running", C.c_int32),
+                ("max_batch", C.c_int32), ("reserved", C.c_int32)]
+
+
 class TrajectoryStats(C.Structure):
     _fields_ = [("segments", C.c_int32), ("passes", C.c_int32), ("mass_passes", C.c_int32),
                 ("waves", C.c_int32), ("batch_states", C.c_int32), ("reserved", C.c_int32),
@@ -132,6 +152,17 @@ SIGNATURES = {
     "qm_plan_stats": (I32, [P, I32P, I32P, I64P]),
     "qm_plan_destroy": (I32, [P]),
     "qm_plan_autotune": (I32, [P, I32, I32, P, I32, I32P, I32, C.POINTER(P), I32P]),
+    "qm_serve_create": (I32, [C.POINTER(ServeOptions), C.POINTER(P)]),
+    "qm_serve_destroy": (I32, [P]),
+    "qm_serve_submit_expectation": (I32, [P, I32, I32, P, I32, P, I32, I64P]),
+    "qm_serve_submit_shots": (I32, [P, I32, I32, P, I32, DP, I32, I64P]),
+    "qm_serve_session_create": (I32, [P, I32, I32, P, I32, I32, P, I32, DP, C.c_double, I64P]),
+    "qm_serve_session_parameters": (I32, [P, I64, DP, I32, I64P]),
+    "qm_serve_session_destroy": (I32, [P, I64]),
+    "qm_serve_submit_vqe_step": (I32, [P, I64, I64P]),
+    "qm_serve_wait": (I32, [P, I64, C.c_double, I32P]),
+    "qm_serve_take_result": (I32, [P, I64, C.POINTER(ServeResult), DP, I32, C.POINTER(C.c_int64), I32, DP, I32]),
+    "qm_serve_get_stats": (I32, [P, C.POINTER(ServeStats)]),
     "qm_graph_create": (I32, [P, P, C.POINTER(P)]),
     "qm_graph_launch": (I32, [P, C.POINTER(Profile)]),
     "qm_graph_destroy": (I32, [P]),

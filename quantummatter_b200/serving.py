@@ -13,34 +13,37 @@ in sequence).  This module serves a stream of such requests concurrently on one 
   steepest-descent update of the session's parameters, which stay resident in the server
   between steps.
 
-Admission: a request reserves the bytes of its state (16 * 2^n for FP64, 8 * 2^n for FP32)
-against the server's budget and waits until the reservation fits; the oldest waiting request
-goes first, and a younger one may pass it only while the older one does not fit.
-Batching: waiting VQE steps whose ansatz structure, Hamiltonian Pauli strings and precision
-match are evaluated as one device batch (qm_vqe_evaluate_coefficients), each with its own
-Hamiltonian coefficients and parameters; a session never has two steps in flight.
-Execution: each worker thread owns a B200Context (its own CUDA stream), so requests on
-different workers overlap on the GPU; a worker keeps the device states of recent sizes for
-reuse instead of allocating one per request.
+The server itself is the library's (qm_serve_* in include/qm_b200.h, csrc/qm_serve.cpp), so a
+.NET host drives the same engine through P/Invoke:
+- admission: a request reserves the bytes of its state (16 * 2^n for FP64, 8 * 2^n for FP32)
+  against the server's budget; the oldest waiting request goes first, and a younger one may pass
+  it only while the older one does not fit;
+- batching: waiting VQE steps whose ansatz structure, Hamiltonian Pauli strings and precision
+  match are evaluated as one device batch (qm_vqe_evaluate_coefficients), each with its own
+  Hamiltonian coefficients and parameters; a session never has two steps in flight;
+- execution: each worker thread owns a context (its own CUDA stream), so requests on different
+  workers overlap on the GPU; a worker keeps the device states of recent sizes for reuse.
+This module holds the request types, the Python face of the server and the plain form.
 """
 from __future__ import annotations
 
+import ctypes as C
 import math
 import threading
 import time
-from collections import deque
-from concurrent.futures import Future
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 from typing import Callable, Sequence
 
 import numpy as np
 
-from .backend import FP32, FP64, B200BackendOptions, B200Context, DeviceState
-from .circuit import QuantumCircuit
+from . import _lib
+from ._lib import check, load
+from .backend import FP32, FP64, B200Context, DeviceState
+from .circuit import QuantumCircuit, operations_array
 from .errors import ArgumentError, ArgumentOutOfRangeError
-from .observables import PauliHamiltonian, PauliString
+from .observables import PauliHamiltonian, PauliString, observable_array, terms_array
 from .trajectories import random_doubles
-from .variational import B200VariationalEnergyEvaluator, ParameterizedCircuit, _fma
+from .variational import ParameterizedCircuit, _fma
 
 
 def state_bytes(qubits: int, precision: int) -> int:
@@ -87,21 +90,7 @@ class VqeSession:
         self.step_size = float(step_size)
         self.precision = precision
         self.steps = 0
-        self.busy = False
-        # requests of sessions with the same key share a device batch
-        self.key = (circuit.QubitCount, precision, _template_key(circuit),
-                    tuple((t.Observable.FlipMask, t.Observable.SignMask, t.Observable.YCount) for t in hamiltonian.Terms))
         self.coefficients = np.array([t.Coefficient for t in hamiltonian.Terms], dtype=np.float64)
-
-
-def _template_key(circuit: ParameterizedCircuit) -> tuple:
-    ops = []
-    for op in circuit.Operations:
-        g = op.Operation
-        u = None if g.Unitary is None else (g.Unitary.M00, g.Unitary.M01, g.Unitary.M10, g.Unitary.M11)
-        ops.append((int(g.Kind), g.Target, g.Control, g.SecondControl, g.Angle if op.ParameterIndex < 0 else None,
-                    op.ParameterIndex, u))
-    return (circuit.ParameterCount, tuple(ops))
 
 
 @dataclass
@@ -137,236 +126,158 @@ class Response:
         return self.finished - self.submitted
 
 
-@dataclass
-class _Item:
-    request: object
-    future: Future
-    submitted: float
-    bytes: int
+class ServeFuture:
+    """A submitted request: result() waits for it and returns its Response (qm_serve_wait,
+    qm_serve_take_result); the request's failure is raised there."""
 
+    def __init__(self, server: "B200Server", request, rid: int, sizes: tuple[int, int, int]):
+        self._server, self._request, self._id, self._sizes = server, request, rid, sizes
+        self._lock = threading.Lock()
+        self._response: Response | None = None
+        self._error: BaseException | None = None
 
-@dataclass
-class Job:
-    items: list[_Item]
-    bytes: int = 0
-    kind: str = ""
+    def done(self) -> bool:
+        if self._response is not None or self._error is not None:
+            return True
+        flag = C.c_int32()
+        check(load().qm_serve_wait(self._server._h, self._id, 0.0, C.byref(flag)))
+        return bool(flag.value)
 
+    def result(self, timeout: float | None = None) -> Response:
+        with self._lock:
+            if self._response is None and self._error is None:
+                deadline = None if timeout is None else time.perf_counter() + timeout
+                flag = C.c_int32()
+                while True:
+                    left = 3600.0 if deadline is None else max(0.0, deadline - time.perf_counter())
+                    check(load().qm_serve_wait(self._server._h, self._id, min(left, 3600.0), C.byref(flag)))
+                    if flag.value:
+                        break
+                    if deadline is not None and time.perf_counter() >= deadline:
+                        raise TimeoutError("the request has not finished")
+                self._take()
+        if self._error is not None:
+            raise self._error
+        return self._response
 
-class Scheduler:
-    """Admission and batching policy (no device work; thread-unsafe, the server locks it)."""
-
-    def __init__(self, budget_bytes: int, max_batch: int = 64, lookahead: int = 64):
-        if budget_bytes <= 0:
-            raise ArgumentOutOfRangeError("budget_bytes")
-        self.budget = int(budget_bytes)
-        self.max_batch = max_batch
-        self.lookahead = lookahead
-        self.reserved = 0
-        self.peak_reserved = 0
-        self.queue: deque[_Item] = deque()
-
-    def push(self, item: _Item) -> None:
-        if item.bytes > self.budget:
-            raise ArgumentOutOfRangeError(f"the request needs {item.bytes} bytes; the budget is {self.budget} bytes")
-        self.queue.append(item)
-
-    def _fits(self, item: _Item) -> bool:
-        return self.reserved + item.bytes <= self.budget
-
-    def _ready(self, item: _Item) -> bool:
-        req = item.request
-        return not (isinstance(req, VqeStepRequest) and req.session.busy)
-
-    def take(self) -> Job | None:
-        """The next job: the oldest ready request that fits (younger ones pass only while the
-        oldest does not fit), plus, for a VQE step, the waiting steps that share its batch key."""
-        pick = None
-        for idx, item in enumerate(self.queue):
-            if idx >= self.lookahead:
-                break
-            if self._ready(item) and self._fits(item):
-                pick = idx
-                break
-        if pick is None:
-            return None
-        head = self.queue[pick]
-        del self.queue[pick]
-        job = Job([head], head.bytes, _kind(head.request))
-        if isinstance(head.request, VqeStepRequest):
-            head.request.session.busy = True
-            key = head.request.session.key
-            rest = deque()
-            while self.queue:
-                item = self.queue.popleft()
-                req = item.request
-                if (len(job.items) < self.max_batch and isinstance(req, VqeStepRequest) and req.session.key == key
-                        and self._ready(item) and self.reserved + job.bytes + item.bytes <= self.budget):
-                    req.session.busy = True
-                    job.items.append(item)
-                    job.bytes += item.bytes
-                else:
-                    rest.append(item)
-            self.queue = rest
-        self.reserved += job.bytes
-        self.peak_reserved = max(self.peak_reserved, self.reserved)
-        return job
-
-    def release(self, job: Job) -> None:
-        self.reserved -= job.bytes
-        for item in job.items:
-            if isinstance(item.request, VqeStepRequest):
-                item.request.session.busy = False
-
-
-def _kind(req) -> str:
-    return {ExpectationRequest: "expectation", ShotsRequest: "shots", VqeStepRequest: "vqe_step"}[type(req)]
-
-
-class _Worker:
-    """Executes jobs on its own context; keeps device states of recent sizes."""
-
-    def __init__(self, context: B200Context, cache_bytes: int):
-        self.context = context
-        self.cache_bytes = cache_bytes
-        self.states: dict[tuple[int, int], DeviceState] = {}
-        self.evaluators: dict[int, B200VariationalEnergyEvaluator] = {}
-
-    def state(self, qubits: int, precision: int) -> DeviceState:
-        key = (qubits, precision)
-        st = self.states.pop(key, None)
-        if st is None:
-            while self.states and sum(state_bytes(q, p) for q, p in self.states) + state_bytes(qubits, precision) > self.cache_bytes:
-                _, old = self.states.popitem()
-                old.Dispose()
-            st = DeviceState(self.context, qubits, precision)
+    def _take(self) -> None:
+        nv, no, np_ = self._sizes
+        values = np.zeros(max(1, nv))
+        outcomes = np.zeros(max(1, no), dtype=np.int64)
+        params = np.zeros(max(1, np_))
+        res = _lib.ServeResult()
+        check(load().qm_serve_take_result(self._server._h, self._id, C.byref(res), values.ctypes.data_as(_lib.DP), nv,
+                                          outcomes.ctypes.data_as(C.POINTER(C.c_int64)), no,
+                                          params.ctypes.data_as(_lib.DP), np_))
+        try:
+            check(res.status)
+        except Exception as e:  # noqa: BLE001 - the request's own failure, raised by result()
+            self._error = e
+            return
+        kind = {0: "expectation", 1: "shots", 2: "vqe_step"}[res.kind]
+        r = Response(kind, batch=res.batch, submitted=res.submitted, started=res.started, finished=res.finished)
+        if kind == "expectation":
+            r.values, r.mass = values[:res.values].copy(), res.mass
+        elif kind == "shots":
+            r.outcomes = outcomes[:res.outcomes].copy()
+            counts: dict[str, int] = {}
+            for o in r.outcomes:
+                k = format(int(o), "b").zfill(self._request.qubits)
+                counts[k] = counts.get(k, 0) + 1
+            r.counts = dict(sorted(counts.items()))
         else:
-            st.Reset()
-        self.states[key] = st  # most recently used last
-        return st
-
-    def run(self, job: Job) -> list[Response]:
-        now = time.perf_counter()
-        if job.kind == "vqe_step":
-            return self._vqe(job, now)
-        item = job.items[0]
-        req = item.request
-        st = self.state(req.qubits, req.precision)
-        st.Evolve(req.circuit)
-        if job.kind == "expectation":
-            values, mass = st.ExpectationValues(list(req.observables))
-            return [Response("expectation", values=values, mass=mass, started=now)]
-        draws = random_doubles(req.seed, req.shots)
-        outcomes, _ = st.Sample(draws)
-        counts: dict[str, int] = {}
-        for o in outcomes:
-            k = format(int(o), "b").zfill(req.qubits)
-            counts[k] = counts.get(k, 0) + 1
-        return [Response("shots", outcomes=outcomes, counts=dict(sorted(counts.items())), started=now)]
-
-    def _vqe(self, job: Job, now: float) -> list[Response]:
-        sessions = [item.request.session for item in job.items]
-        s0 = sessions[0]
-        ev = self.evaluators.get(s0.precision)
-        if ev is None:
-            ev = self.evaluators[s0.precision] = B200VariationalEnergyEvaluator(self.context, s0.precision)
-        params = np.stack([s.parameters for s in sessions])
-        coef = np.stack([s.coefficients for s in sessions])
-        r = ev.EvaluateBatch(s0.circuit, s0.hamiltonian, params, withGradient=True, coefficients=coef)
-        out = []
-        for i, s in enumerate(sessions):
-            g = r.Gradients[i]
-            s.parameters = np.array([_fma(-s.step_size, float(gi), float(pi)) for gi, pi in zip(g, s.parameters)])
+            r.energy, r.gradient = res.energy, values[:res.values].copy()
+            r.parameters = params[:res.parameters].copy()
+            s = self._request.session
+            s.parameters = r.parameters.copy()
             s.steps += 1
-            out.append(Response("vqe_step", energy=float(r.Energies[i]), gradient=g.copy(),
-                                parameters=s.parameters.copy(), batch=len(sessions), started=now))
-        return out
+        self._response = r
 
 
 class B200Server:
-    """Serves requests from `workers` threads, each with its own context and stream."""
+    """The library's request server (qm_serve_*): `workers` threads, each with its own context and
+    CUDA stream, admission by state bytes against `budget_bytes`, batched VQE steps."""
 
     def __init__(self, workers: int = 4, budget_bytes: int = 64 << 30, max_batch: int = 64,
-                 context_budget_bytes: int = 32 << 30, cache_bytes: int = 8 << 30, device_index: int = 0,
-                 contexts: Sequence[B200Context] | None = None):
+                 context_budget_bytes: int = 32 << 30, cache_bytes: int = 8 << 30, device_index: int = 0):
         if workers < 1:
             raise ArgumentOutOfRangeError("workers")
-        self.scheduler = Scheduler(budget_bytes, max_batch)
-        self._cv = threading.Condition()
-        self._closed = False
-        own = contexts is None
-        if own:
-            contexts = [B200Context(B200BackendOptions(DeviceIndex=device_index,
-                                                       DeviceMemoryBudgetBytes=context_budget_bytes,
-                                                       StagingMemoryBudgetBytes=1 << 30))
-                        for _ in range(workers)]
-        self._own = own
-        self._workers = [_Worker(c, cache_bytes) for c in contexts]
-        self._threads = [threading.Thread(target=self._loop, args=(w,), daemon=True) for w in self._workers]
-        self.completed = 0
-        for t in self._threads:
-            t.start()
+        o = _lib.ServeOptions()
+        o.device_index, o.workers, o.budget_bytes = device_index, workers, budget_bytes
+        o.context_budget_bytes, o.cache_bytes, o.max_batch = context_budget_bytes, cache_bytes, max_batch
+        h = C.c_void_p()
+        check(load().qm_serve_create(C.byref(o), C.byref(h)))
+        self._h = h
+        self._sessions: dict[int, int] = {}  # id(VqeSession) -> server session
+        self._session_objects: dict[int, VqeSession] = {}
 
-    def submit(self, request) -> Future:
-        if not isinstance(request, (ExpectationRequest, ShotsRequest, VqeStepRequest)):
+    def _session(self, s: VqeSession) -> int:
+        sid = self._sessions.get(id(s))
+        if sid is None:
+            ops, nops = s.circuit.template_array()
+            arr, n = terms_array(s.hamiltonian.Terms)
+            params = np.ascontiguousarray(s.parameters, dtype=np.float64)
+            out = C.c_int64()
+            check(load().qm_serve_session_create(self._h, s.circuit.QubitCount, s.precision, ops, nops,
+                                                 s.circuit.ParameterCount, arr, n, params.ctypes.data_as(_lib.DP),
+                                                 s.step_size, C.byref(out)))
+            sid = self._sessions[id(s)] = out.value
+            self._session_objects[id(s)] = s
+        return sid
+
+    def submit(self, request) -> ServeFuture:
+        rid = C.c_int64()
+        if isinstance(request, ExpectationRequest):
+            ops, n = operations_array(request.circuit.Operations)
+            arr, t = observable_array(list(request.observables))
+            check(load().qm_serve_submit_expectation(self._h, request.qubits, request.precision, ops, n, arr, t,
+                                                     C.byref(rid)))
+            sizes = (t, 0, 0)
+        elif isinstance(request, ShotsRequest):
+            ops, n = operations_array(request.circuit.Operations)
+            draws = np.ascontiguousarray(random_doubles(request.seed, request.shots), dtype=np.float64)
+            check(load().qm_serve_submit_shots(self._h, request.qubits, request.precision, ops, n,
+                                               draws.ctypes.data_as(_lib.DP), request.shots, C.byref(rid)))
+            sizes = (0, request.shots, 0)
+        elif isinstance(request, VqeStepRequest):
+            sid = self._session(request.session)
+            check(load().qm_serve_submit_vqe_step(self._h, sid, C.byref(rid)))
+            p = request.session.circuit.ParameterCount
+            sizes = (p, 0, p)
+        else:
             raise ArgumentError("unknown request")
-        fut: Future = Future()
-        item = _Item(request, fut, time.perf_counter(), state_bytes(request.qubits, request.precision))
-        with self._cv:
-            if self._closed:
-                raise ArgumentError("the server is closed")
-            self.scheduler.push(item)
-            self._cv.notify_all()
-        return fut
+        return ServeFuture(self, request, rid.value, sizes)
 
-    def _loop(self, worker: _Worker) -> None:
-        while True:
-            with self._cv:
-                job = None
-                while not self._closed:
-                    job = self.scheduler.take()
-                    if job is not None:
-                        break
-                    self._cv.wait()
-                if job is None:
-                    return
-            try:
-                responses = worker.run(job)
-                error = None
-            except Exception as e:  # the request's caller sees the failure
-                responses, error = None, e
-            done = time.perf_counter()
-            with self._cv:
-                self.scheduler.release(job)
-                self.completed += len(job.items)
-                self._cv.notify_all()
-            for i, item in enumerate(job.items):
-                if error is not None:
-                    item.future.set_exception(error)
-                    continue
-                r = responses[i]
-                r.submitted = item.submitted
-                r.finished = done
-                item.future.set_result(r)
+    def stats(self) -> dict:
+        st = _lib.ServeStats()
+        check(load().qm_serve_get_stats(self._h, C.byref(st)))
+        return {name: getattr(st, name) for name, _ in _lib.ServeStats._fields_}
 
     def close(self) -> None:
-        with self._cv:
-            self._closed = True
-            self._cv.notify_all()
-        for t in self._threads:
-            t.join()
-        for w in self._workers:
-            for st in w.states.values():
-                st.Dispose()
-            w.states.clear()
-        if self._own:
-            for w in self._workers:
-                w.context.Dispose()
+        if self._h is None:
+            return
+        # sessions whose last results were never taken still get their parameters back
+        for key, sid in self._sessions.items():
+            s = self._session_objects[key]
+            params = np.zeros(max(1, s.circuit.ParameterCount))
+            steps = C.c_int64()
+            if load().qm_serve_session_parameters(self._h, sid, params.ctypes.data_as(_lib.DP), len(params),
+                                                  C.byref(steps)) == 0 and steps.value > s.steps:
+                s.parameters, s.steps = params[:s.circuit.ParameterCount].copy(), steps.value
+        load().qm_serve_destroy(self._h)
+        self._h = None
 
     def __enter__(self):
         return self
 
     def __exit__(self, *exc):
         self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def serve_plain(requests: Sequence, context: B200Context,

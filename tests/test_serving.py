@@ -53,7 +53,9 @@ def test_mixed_results_equal_alone(gpu_context, precision):
     budget = 6 * state_bytes(12, FP64)
     with B200Server(workers=3, budget_bytes=budget, context_budget_bytes=2 << 30, cache_bytes=1 << 28) as server:
         mixed, mixed_vqe = run(server, reqs, sessions)
-        assert server.scheduler.peak_reserved <= budget
+        stats = server.stats()
+        assert 0 < stats["peak_reserved_bytes"] <= budget
+        assert stats["completed"] == len(reqs) + 2 * len(sessions) and stats["max_batch"] >= 2
     assert max(r.batch for row in mixed_vqe for r in row) >= 2  # VQE steps were batched
     alone_sessions = make_sessions(precision)
     with B200Server(workers=1, budget_bytes=budget, context_budget_bytes=2 << 30) as server:
