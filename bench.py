@@ -370,6 +370,7 @@ def run_vqe(args) -> None:
     total_circuits = 0
     max_de = 0.0
     timings = {"fp32": 0.0, "fp64": 0.0}
+    per_size_energies = {}
     for n in sizes:
         c = hardware_efficient_ansatz(n, 4)
         h = xxz_chain(n)
@@ -377,7 +378,7 @@ def run_vqe(args) -> None:
         per = {}
         for name, prec in (("fp32", FP32), ("fp64", FP64)):
             ev = B200VariationalEnergyEvaluator(ctx, prec)
-            ev.EvaluateBatch(c, h, params[:2], withGradient=True)  # warm-up (plans, kernel attributes)
+            ev.EvaluateBatch(c, h, params, withGradient=True)  # warm-up: plans, kernel attributes, graph capture
             t0 = time.perf_counter()
             r = ev.EvaluateBatch(c, h, params, withGradient=True)
             dt = time.perf_counter() - t0
@@ -386,12 +387,26 @@ def run_vqe(args) -> None:
             results[f"n{n}_{name}"] = {"seconds": dt, "circuits": r.Circuits, "evals_per_s": r.Circuits / dt,
                                        "waves": r.Waves, "batch_states": r.BatchStates,
                                        "passes_per_circuit": r.PassesPerCircuit, "tile_passes": r.TilePasses}
+        per_size_energies[n] = per["fp32"].Energies
         de = float(np.max(np.abs(per["fp32"].Energies - per["fp64"].Energies)))
         dg = float(np.max(np.abs(per["fp32"].Gradients - per["fp64"].Gradients)))
         results[f"n{n}_fp32_max_abs_dE"] = de
         results[f"n{n}_fp32_max_abs_dgrad"] = dg
         max_de = max(max_de, de)
         total_circuits += per["fp64"].Circuits
+    # every size in one call: each round's waves of all sizes on their own streams, one graph launch
+    mixed_problems = []
+    for n in sizes:
+        c = hardware_efficient_ansatz(n, 4)
+        mixed_problems.append((c, xxz_chain(n), uniform_parameters(c.ParameterCount, args.vectors, -np.pi, np.pi,
+                                                                    seed=n)))
+    ev32 = B200VariationalEnergyEvaluator(ctx, FP32)
+    ev32.EvaluateMixed([(c, h, p[:2]) for c, h, p in mixed_problems])  # warm-up
+    t0 = time.perf_counter()
+    mixed_outs, mixed_total = ev32.EvaluateMixed(mixed_problems)
+    mixed_dt = time.perf_counter() - t0
+    mixed_equal = all(np.array_equal(o[0], results_e) for o, results_e in
+                      zip(mixed_outs, [per_size_energies[n] for n in sizes]))
     # plain form: one FP64 circuit at a time, resident state, per-term energy on the device
     n = sizes[-1]
     c = hardware_efficient_ansatz(n, 4)
@@ -417,6 +432,12 @@ def run_vqe(args) -> None:
                                f"sizes {sizes}, {args.vectors} vectors each, full parameter-shift gradients",
                    "circuits": total_circuits},
         "fp64_value": total_circuits / timings["fp64"],
+        "mixed_fp32_evals_per_s": mixed_total.Circuits / mixed_dt,
+        "mixed_fp32": {"rounds": mixed_total.Waves, "batch_states": mixed_total.BatchStates,
+                       "device_seconds": mixed_total.DeviceSeconds, "wall_seconds": mixed_dt,
+                       "energies_equal_per_size_runs": bool(mixed_equal),
+                       "form": "all sizes in one qm_vqe_evaluate_mixed call: each round one graph launch with a "
+                               "branch per size"},
         "fp32_max_abs_dE_vs_fp64": max_de,
         f"plain_fp64_evals_per_s_n{n}": 1.0 / plain_dt,
         f"batched_fp32_over_plain_n{n}": batched_n * plain_dt,

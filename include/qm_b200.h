@@ -409,6 +409,28 @@ int32_t qm_vqe_evaluate_coefficients(qm_context* context, int32_t qubits, int32_
                                      const double* parameters, int32_t vectors, int32_t with_gradient,
                                      double* energies, double* gradients, qm_vqe_stats* stats);
 
+/* Several evaluations of different sizes at once (the batched form of VariationalEnergyEvaluator
+ * for a mix of registers, e.g. 16-, 18-, 20- and 22-qubit ansatzes).  Each problem is what one
+ * qm_vqe_evaluate / qm_vqe_evaluate_coefficients call takes (coefficients NULL: the terms' own).
+ * The device budget is shared in proportion to each problem's state bytes; every round runs each
+ * problem's next wave on its own stream, forked from and joined to the context's stream, so the
+ * sizes overlap on the device, and rounds in which every problem runs a full wave replay one
+ * captured CUDA graph (one launch for all sizes).  Results equal the separate calls'. */
+typedef struct qm_vqe_problem {
+    int32_t qubits, precision;
+    const qm_template_op* operations;
+    int32_t operation_count, parameter_count;
+    const qm_pauli_term* terms;
+    int32_t term_count, vectors;
+    const double* coefficients;     /* [vectors][term_count] or NULL */
+    const double* parameters;       /* [vectors][parameter_count] */
+    int32_t with_gradient, reserved;
+    double* energies;               /* [vectors] */
+    double* gradients;              /* [vectors][parameter_count] when with_gradient */
+} qm_vqe_problem;                   /* 80 bytes */
+int32_t qm_vqe_evaluate_mixed(qm_context* context, const qm_vqe_problem* problems, int32_t count,
+                              qm_vqe_stats* stats);
+
 /* ---------------------------------------------------------------- serving */
 
 /* A request server on one GPU; no reference counterpart (applications call the reference's port

@@ -89,6 +89,14 @@ class TrajectoryOutputs(C.Structure):
                 ("probability_means", C.POINTER(C.c_double)), ("probability_stderr", C.POINTER(C.c_double))]
 
 
+class VqeProblem(C.Structure):
+    _fields_ = [("qubits", C.c_int32), ("precision", C.c_int32), ("operations", C.c_void_p),
+                ("operation_count", C.c_int32), ("parameter_count", C.c_int32), ("terms", C.c_void_p),
+                ("term_count", C.c_int32), ("vectors", C.c_int32), ("coefficients", C.POINTER(C.c_double)),
+                ("parameters", C.POINTER(C.c_double)), ("with_gradient", C.c_int32), ("reserved", C.c_int32),
+                ("energies", C.POINTER(C.c_double)), ("gradients", C.POINTER(C.c_double))]
+
+
 class ServeOptions(C.Structure):
     _fields_ = [("device_index", C.c_int32), ("workers", C.c_int32), ("budget_bytes", C.c_int64),
                 ("context_budget_bytes", C.c_int64), ("cache_bytes", C.c_int64), ("max_batch", C.c_int32),
@@ -152,6 +160,7 @@ SIGNATURES = {
     "qm_plan_stats": (I32, [P, I32P, I32P, I64P]),
     "qm_plan_destroy": (I32, [P]),
     "qm_plan_autotune": (I32, [P, I32, I32, P, I32, I32P, I32, C.POINTER(P), I32P]),
+    "qm_vqe_evaluate_mixed": (I32, [P, C.POINTER(VqeProblem), I32, C.POINTER(VqeStats)]),
     "qm_serve_create": (I32, [C.POINTER(ServeOptions), C.POINTER(P)]),
     "qm_serve_destroy": (I32, [P]),
     "qm_serve_submit_expectation": (I32, [P, I32, I32, P, I32, P, I32, I64P]),

@@ -404,129 +404,166 @@ void neumaier_add(double& sum, double& correction, double value) {
 
 namespace {
 
+// One parameter-shift evaluation problem: a template, a Hamiltonian and `vectors` parameter
+// vectors; every base and shifted circuit is a state of this problem's device batch.
 // coefficients: [vectors][term_count] per-vector term coefficients, or null for the terms' own.
-int32_t vqe_evaluate(qm_context* ctx, int32_t qubits, int32_t precision, const qm_template_op* ops, int32_t op_count,
-                     int32_t parameter_count, const qm_pauli_term* terms, int32_t term_count, const double* coefficients,
-                     const double* parameters, int32_t vectors, int32_t with_gradient, double* energies,
-                     double* gradients, qm_vqe_stats* stats) {
-    auto wall0 = std::chrono::steady_clock::now();
-    if (!ctx) return fail(QM_E_ARG, "context is null");
-    if (qubits < 1 || qubits > 30) return fail(QM_E_RANGE, "qubits must be between 1 and 30");
-    if (precision != QM_FP64 && precision != QM_FP32) return fail(QM_E_RANGE, "unknown precision");
-    if (op_count < 0 || (op_count > 0 && !ops)) return fail(QM_E_ARG, "template is null");
-    if (parameter_count < 0) return fail(QM_E_RANGE, "parameter count must be nonnegative");
-    if (vectors < 1) return fail(QM_E_RANGE, "vectors must be positive");
-    if (!parameters && parameter_count > 0) return fail(QM_E_ARG, "parameters is null");
-    if (!energies) return fail(QM_E_ARG, "energies is null");
-    if (with_gradient && parameter_count > 0 && !gradients) return fail(QM_E_ARG, "gradients is null");
-    if (term_count < 0 || (term_count > 0 && !terms)) return fail(QM_E_ARG, "terms is null");
-    const uint32_t all = (uint32_t)((1ull << qubits) - 1);
-    for (int32_t t = 0; t < term_count; ++t) {
-        if ((terms[t].flip_mask | terms[t].sign_mask) & ~all) return fail(QM_E_ARG, "Circuit and Hamiltonian sizes must match.");
-        if (!coefficients && !std::isfinite(terms[t].coefficient)) return fail(QM_E_RANGE, "coefficient must be finite");
-    }
-    if (coefficients)
-        for (int64_t i = 0; i < (int64_t)vectors * term_count; ++i)
-            if (!std::isfinite(coefficients[i])) return fail(QM_E_RANGE, "coefficient must be finite");
-    auto coef = [&](int v, int t) {
-        return coefficients ? coefficients[(size_t)v * term_count + t] : terms[t].coefficient;
-    };
-    for (int64_t i = 0; i < (int64_t)vectors * parameter_count; ++i)
-        if (!std::isfinite(parameters[i])) return fail(QM_E_RANGE, "Parameters must be finite.");
-
-    // template: constant gates prepared once; rotations get one coefficient slot each
-    std::vector<qm_gate> gates((size_t)op_count);
-    std::vector<int32_t> slots((size_t)op_count, -1);
+struct VqeProblem {
+    // inputs
+    int32_t qubits = 0, precision = QM_FP64;
+    const qm_template_op* ops = nullptr;
+    int32_t op_count = 0, parameter_count = 0;
+    const qm_pauli_term* terms = nullptr;
+    int32_t term_count = 0;
+    const double* coefficients = nullptr;
+    const double* parameters = nullptr;
+    int32_t vectors = 0, with_gradient = 0;
+    double* energies = nullptr;
+    double* gradients = nullptr;
+    // derived
+    std::vector<qm_gate> gates;
+    std::vector<int32_t> slots;
     std::vector<Rotation> rot;
-    for (int32_t i = 0; i < op_count; ++i) {
-        const qm_template_op& t = ops[i];
-        if (t.parameter >= 0) {
-            if (t.parameter >= parameter_count) return fail(QM_E_RANGE, "parameter index out of range");
-            const int k = t.operation.kind;
-            if ((k != QM_GATE_RX && k != QM_GATE_RY && k != QM_GATE_RZ) || t.operation.control != -1 ||
-                t.operation.second_control != -1)
-                return fail(QM_E_ARG, "parameterized operations are uncontrolled Rx, Ry or Rz");
-            qm_operation rep = t.operation;
-            rep.angle = 1.0;  // fixes the kernel kind (real matrix, complex matrix or diagonal)
-            int32_t rc = qm_prepare_gates(&rep, 1, qubits, &gates[(size_t)i]);
-            if (rc) return rc;
-            slots[(size_t)i] = (int32_t)rot.size();
-            rot.push_back(Rotation{i, t.parameter, k});
-        } else {
-            int32_t rc = qm_prepare_gates(&t.operation, 1, qubits, &gates[(size_t)i]);
-            if (rc) return rc;
-        }
-    }
-    const int R = (int)rot.size();
-    const int per_vector = with_gradient ? 1 + 2 * R : 1;
-    const int64_t circuits = (int64_t)vectors * per_vector;
-    const int slot_count = std::max(R, 1);
-    // Registers below the 9-qubit minimum block run embedded in 9 qubits: the extra qubits stay
-    // |0> and no term touches them, so energies and gradients are those of the small register.
-    qubits = std::max(qubits, 9);
-
-    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
-    if (ctx->disposed) return fail(QM_E_DISPOSED, "context disposed");
-    QM_CUDA(cudaSetDevice(ctx->device));
+    int R = 0, per_vector = 1, slot_count = 1;
+    int64_t circuits = 0;
+    int32_t exec_qubits = 0;
     Plan plan;
-    std::string err;
-    if (!plan_fused(gates, qubits, precision, ctx->fusion_width, plan, err, &slots)) return fail(QM_E_ARG, "planner: " + err);
-    struct Release {
-        Plan& p;
-        ~Release() { plan_release(p); }
-    } release{plan};
-    {
-        plan.start_zero = true;  // every circuit starts from |0...0>
-        jit_prepare(plan);       // one structure for every circuit of every wave
-        int32_t urc = plan_upload(plan, ctx->stream);
-        if (urc) return urc;
-    }
     TilePlan tp;
-    if (!plan_tiles(qubits, precision, terms, term_count, tp, err)) return fail(QM_E_ARG, err);
-    jit_prepare_tiles(tp, qubits, precision);  // one term list for every circuit of every wave
-
-    const int64_t state_bytes = (precision == QM_FP32 ? 8ll : 16ll) << qubits;
-    const int64_t free_budget = ctx->device_budget - ctx->device_in_use;
-    int64_t cap = std::min<int64_t>({circuits, 65535, free_budget / std::max<int64_t>(state_bytes, 1), 8192});
-    if (cap < 1) return fail(QM_E_BUDGET, "a single state exceeds the context's device memory budget");
     qm_batch* batch = nullptr;
-    int32_t rc = qm_batch_create(ctx, qubits, precision, (int32_t)cap, &batch);
-    if (rc) return rc;
-    std::unique_ptr<qm_batch, int32_t (*)(qm_batch*)> guard(batch, qm_batch_destroy);
-    const int B = (int)cap;
-    const size_t table_doubles = (size_t)B * slot_count * 8;
-    rc = grow(batch->table, batch->table_bytes, sizeof(double) * table_doubles);
-    if (rc) return rc;
-
+    int B = 0;
     double* h_table[2] = {nullptr, nullptr};
     double* h_out[2] = {nullptr, nullptr};
-    struct PinnedGuard {
-        double** p;
-        int n;
-        ~PinnedGuard() {
-            for (int i = 0; i < n; ++i)
-                if (p[i]) cudaFreeHost(p[i]);
-        }
-    } g1{h_table, 2}, g2{h_out, 2};
-    for (int i = 0; i < 2; ++i) {
-        QM_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h_table[i]), sizeof(double) * table_doubles));
-        QM_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h_out[i]), sizeof(double) * (size_t)B * tp.columns));
-    }
-
-    // base coefficients of every rotation of every vector, and the two shift matrices per kind
-    const double half_pi = M_PI / 2;
+    std::vector<double> base;
+    std::vector<double> results;
     double shift_plus[3][8], shift_minus[3][8];
-    for (int k = 0; k < 3; ++k) {
-        rotation_coefficients(QM_GATE_RX + k, half_pi, shift_plus[k]);
-        rotation_coefficients(QM_GATE_RX + k, -half_pi, shift_minus[k]);
-    }
-    std::vector<double> base((size_t)vectors * slot_count * 8, 0.0);
-    for (int v = 0; v < vectors; ++v)
-        for (int r = 0; r < R; ++r)
-            rotation_coefficients(rot[(size_t)r].kind, parameters[(size_t)v * parameter_count + rot[(size_t)r].parameter],
-                                  &base[((size_t)v * slot_count + r) * 8]);
+    int64_t pending_first[2] = {-1, -1};
+    int pending_count[2] = {0, 0};
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
 
-    auto fill_table = [&](double* dst, int64_t first, int count) {
+    VqeProblem() = default;
+    VqeProblem(const VqeProblem&) = delete;
+    VqeProblem& operator=(const VqeProblem&) = delete;
+    ~VqeProblem() {
+        plan_release(plan);
+        for (int i = 0; i < 2; ++i) {
+            if (h_table[i]) cudaFreeHost(h_table[i]);
+            if (h_out[i]) cudaFreeHost(h_out[i]);
+        }
+        if (batch) qm_batch_destroy(batch);
+        if (own_stream && stream) cudaStreamDestroy(stream);
+    }
+
+    double coef(int v, int t) const {
+        return coefficients ? coefficients[(size_t)v * term_count + t] : terms[t].coefficient;
+    }
+    int64_t state_bytes() const { return (precision == QM_FP32 ? 8ll : 16ll) << exec_qubits; }
+    int64_t waves() const { return B ? (circuits + B - 1) / B : 0; }
+
+    // Arguments, template and coefficients (host only).
+    int32_t validate() {
+        if (qubits < 1 || qubits > 30) return fail(QM_E_RANGE, "qubits must be between 1 and 30");
+        if (precision != QM_FP64 && precision != QM_FP32) return fail(QM_E_RANGE, "unknown precision");
+        if (op_count < 0 || (op_count > 0 && !ops)) return fail(QM_E_ARG, "template is null");
+        if (parameter_count < 0) return fail(QM_E_RANGE, "parameter count must be nonnegative");
+        if (vectors < 1) return fail(QM_E_RANGE, "vectors must be positive");
+        if (!parameters && parameter_count > 0) return fail(QM_E_ARG, "parameters is null");
+        if (!energies) return fail(QM_E_ARG, "energies is null");
+        if (with_gradient && parameter_count > 0 && !gradients) return fail(QM_E_ARG, "gradients is null");
+        if (term_count < 0 || (term_count > 0 && !terms)) return fail(QM_E_ARG, "terms is null");
+        const uint32_t all = (uint32_t)((1ull << qubits) - 1);
+        for (int32_t t = 0; t < term_count; ++t) {
+            if ((terms[t].flip_mask | terms[t].sign_mask) & ~all)
+                return fail(QM_E_ARG, "Circuit and Hamiltonian sizes must match.");
+            if (!coefficients && !std::isfinite(terms[t].coefficient)) return fail(QM_E_RANGE, "coefficient must be finite");
+        }
+        if (coefficients)
+            for (int64_t i = 0; i < (int64_t)vectors * term_count; ++i)
+                if (!std::isfinite(coefficients[i])) return fail(QM_E_RANGE, "coefficient must be finite");
+        for (int64_t i = 0; i < (int64_t)vectors * parameter_count; ++i)
+            if (!std::isfinite(parameters[i])) return fail(QM_E_RANGE, "Parameters must be finite.");
+        // template: constant gates prepared once; rotations get one coefficient slot each
+        gates.assign((size_t)op_count, qm_gate{});
+        slots.assign((size_t)op_count, -1);
+        rot.clear();
+        for (int32_t i = 0; i < op_count; ++i) {
+            const qm_template_op& t = ops[i];
+            if (t.parameter >= 0) {
+                if (t.parameter >= parameter_count) return fail(QM_E_RANGE, "parameter index out of range");
+                const int k = t.operation.kind;
+                if ((k != QM_GATE_RX && k != QM_GATE_RY && k != QM_GATE_RZ) || t.operation.control != -1 ||
+                    t.operation.second_control != -1)
+                    return fail(QM_E_ARG, "parameterized operations are uncontrolled Rx, Ry or Rz");
+                qm_operation rep = t.operation;
+                rep.angle = 1.0;  // fixes the kernel kind (real matrix, complex matrix or diagonal)
+                int32_t rc = qm_prepare_gates(&rep, 1, qubits, &gates[(size_t)i]);
+                if (rc) return rc;
+                slots[(size_t)i] = (int32_t)rot.size();
+                rot.push_back(Rotation{i, t.parameter, k});
+            } else {
+                int32_t rc = qm_prepare_gates(&t.operation, 1, qubits, &gates[(size_t)i]);
+                if (rc) return rc;
+            }
+        }
+        R = (int)rot.size();
+        per_vector = with_gradient ? 1 + 2 * R : 1;
+        circuits = (int64_t)vectors * per_vector;
+        slot_count = std::max(R, 1);
+        // Registers below the 9-qubit minimum block run embedded in 9 qubits: the extra qubits stay
+        // |0> and no term touches them, so energies and gradients are those of the small register.
+        exec_qubits = std::max(qubits, 9);
+        return QM_OK;
+    }
+
+    // Schedule, compiled passes and tile plan (context locked).
+    int32_t prepare(qm_context* ctx) {
+        std::string err;
+        if (!plan_fused(gates, exec_qubits, precision, ctx->fusion_width, plan, err, &slots))
+            return fail(QM_E_ARG, "planner: " + err);
+        plan.start_zero = true;  // every circuit starts from |0...0>
+        jit_prepare(plan);       // one structure for every circuit of every wave
+        int32_t rc = plan_upload(plan, ctx->stream);
+        if (rc) return rc;
+        if (!plan_tiles(exec_qubits, precision, terms, term_count, tp, err)) return fail(QM_E_ARG, err);
+        jit_prepare_tiles(tp, exec_qubits, precision);  // one term list for every circuit of every wave
+        const double half_pi = M_PI / 2;
+        for (int k = 0; k < 3; ++k) {
+            rotation_coefficients(QM_GATE_RX + k, half_pi, shift_plus[k]);
+            rotation_coefficients(QM_GATE_RX + k, -half_pi, shift_minus[k]);
+        }
+        base.assign((size_t)vectors * slot_count * 8, 0.0);
+        for (int v = 0; v < vectors; ++v)
+            for (int r = 0; r < R; ++r)
+                rotation_coefficients(rot[(size_t)r].kind,
+                                      parameters[(size_t)v * parameter_count + rot[(size_t)r].parameter],
+                                      &base[((size_t)v * slot_count + r) * 8]);
+        results.assign((size_t)circuits * tp.columns, 0.0);
+        return QM_OK;
+    }
+
+    // The device batch: as many states as `bytes` allow (at least one), its table, tile partials
+    // and pinned host buffers, all at full size before any capture.
+    int32_t allocate(qm_context* ctx, int64_t bytes) {
+        const int64_t cap = std::min<int64_t>({circuits, 65535, bytes / std::max<int64_t>(state_bytes(), 1), 8192});
+        if (cap < 1) return fail(QM_E_BUDGET, "a single state exceeds the context's device memory budget");
+        int32_t rc = qm_batch_create(ctx, exec_qubits, precision, (int32_t)cap, &batch);
+        if (rc) return rc;
+        B = (int)cap;
+        const size_t table_doubles = (size_t)B * slot_count * 8;
+        rc = grow(batch->table, batch->table_bytes, sizeof(double) * table_doubles);
+        if (rc) return rc;
+        rc = grow(batch->partials, batch->partial_bytes, sizeof(double) * (size_t)B * tp.rows_per_state * tp.columns);
+        if (rc) return rc;
+        rc = grow(batch->out, batch->out_bytes, sizeof(double) * (size_t)B * tp.columns);
+        if (rc) return rc;
+        for (int i = 0; i < 2; ++i) {
+            QM_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h_table[i]), sizeof(double) * table_doubles));
+            QM_CUDA(cudaMallocHost(reinterpret_cast<void**>(&h_out[i]), sizeof(double) * (size_t)B * tp.columns));
+        }
+        return QM_OK;
+    }
+
+    void fill_table(int buf, int64_t first, int count) {
+        double* dst = h_table[buf];
         for (int i = 0; i < count; ++i) {
             const int64_t c = first + i;
             const int v = (int)(c / per_vector), which = (int)(c % per_vector);
@@ -541,47 +578,177 @@ int32_t vqe_evaluate(qm_context* ctx, int32_t qubits, int32_t precision, const q
                 cmat(shift, shift + 2, shift + 4, shift + 6, m, m + 2, m + 4, m + 6, row + (size_t)r * 8);
             }
         }
-    };
+    }
 
-    // raw per-term sums and masses of every circuit
-    std::vector<double> results((size_t)circuits * tp.columns);
-    cudaStream_t st = ctx->stream;
-    cudaEvent_t done[2], e0, e1;
-    QM_CUDA(cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming));
-    QM_CUDA(cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming));
-    QM_CUDA(cudaEventCreate(&e0));
-    QM_CUDA(cudaEventCreate(&e1));
-    struct EventGuard {
-        cudaEvent_t* e;
-        ~EventGuard() {
-            for (int i = 0; i < 4; ++i) cudaEventDestroy(e[i]);
-        }
-    };
-    cudaEvent_t evs[4] = {done[0], done[1], e0, e1};
-    EventGuard eg{evs};
-
-    // tile partial buffers at full size before any capture
-    rc = grow(batch->partials, batch->partial_bytes, sizeof(double) * (size_t)B * tp.rows_per_state * tp.columns);
-    if (rc) return rc;
-    rc = grow(batch->out, batch->out_bytes, sizeof(double) * (size_t)B * tp.columns);
-    if (rc) return rc;
-
-    auto enqueue_wave = [&](int buf, int count) -> int32_t {
+    // Coefficient upload, evolution from |0...0>, tiled expectation and the download of the raw
+    // sums of `count` circuits, on stream st (capturable: no allocation, no synchronisation).
+    int32_t enqueue_wave(int buf, int count, cudaStream_t st) {
         QM_CUDA(cudaMemcpyAsync(batch->table, h_table[buf], sizeof(double) * (size_t)count * slot_count * 8,
                                 cudaMemcpyHostToDevice, st));
-        if (!plan.zero_fused) QM_CUDA(launch_reset_batched(batch->amps, qubits, precision, count, st));
-        int32_t r2 = enqueue_plan(batch, plan, count, batch->table, (size_t)slot_count * 8, st);
-        if (r2) return r2;
-        r2 = enqueue_tiles(batch, tp, count, st);
-        if (r2) return r2;
+        if (!plan.zero_fused) QM_CUDA(launch_reset_batched(batch->amps, exec_qubits, precision, count, st));
+        int32_t rc = enqueue_plan(batch, plan, count, batch->table, (size_t)slot_count * 8, st);
+        if (rc) return rc;
+        rc = enqueue_tiles(batch, tp, count, st);
+        if (rc) return rc;
         QM_CUDA(cudaMemcpyAsync(h_out[buf], batch->out, sizeof(double) * (size_t)count * tp.columns,
                                 cudaMemcpyDeviceToHost, st));
         return QM_OK;
-    };
+    }
 
-    // full waves replay a captured CUDA graph (one graph per host buffer); the last, partial
-    // wave is launched directly
-    const int64_t waves = (circuits + B - 1) / B;
+    // after the wave's completion event: its sums into the results
+    void collect(int buf) {
+        if (pending_first[buf] < 0) return;
+        std::memcpy(&results[(size_t)pending_first[buf] * tp.columns], h_out[buf],
+                    sizeof(double) * (size_t)pending_count[buf] * tp.columns);
+        pending_first[buf] = -1;
+    }
+
+    // energies and gradients in the reference's order (StateVector.Energy.cs:22-45,
+    // VariationalEnergyEvaluator.cs:45-85)
+    int32_t assemble() {
+        auto value = [&](int64_t c, int t, double& out) -> bool {
+            const double mass = results[(size_t)c * tp.columns + tp.mass_column];
+            const double raw = results[(size_t)c * tp.columns + t];
+            if (!std::isfinite(mass) || mass <= 0 || !std::isfinite(raw)) return false;
+            out = raw / mass;
+            return true;
+        };
+        for (int v = 0; v < vectors; ++v) {
+            const int64_t c0 = (int64_t)v * per_vector;
+            {
+                const double mass = results[(size_t)c0 * tp.columns + tp.mass_column];
+                if (!std::isfinite(mass) || mass <= 0)
+                    return fail(QM_E_MASS, "The state has no finite positive probability mass.");
+            }
+            double sum = 0, corr = 0;
+            for (int t = 0; t < term_count; ++t) {
+                const double ct = coef(v, t);
+                if (ct == 0) continue;
+                double e;
+                if (!value(c0, t, e)) return fail(QM_E_MASS, "The observable accumulation is nonfinite.");
+                neumaier_add(sum, corr, ct * e);
+                if (!std::isfinite(sum) || !std::isfinite(corr))
+                    return fail(QM_E_MASS, "The energy accumulation is nonfinite.");
+            }
+            const double energy = sum + corr;
+            if (!std::isfinite(energy)) return fail(QM_E_MASS, "The energy is nonfinite.");
+            energies[v] = energy;
+            if (!with_gradient) continue;
+            double* grad = gradients + (size_t)v * parameter_count;
+            std::vector<double> correction((size_t)parameter_count, 0.0);
+            for (int p = 0; p < parameter_count; ++p) grad[p] = 0.0;
+            for (int r = 0; r < R; ++r) {
+                const int64_t cp = c0 + 1 + 2 * r, cm = cp + 1;
+                for (int64_t c : {cp, cm}) {
+                    const double mass = results[(size_t)c * tp.columns + tp.mass_column];
+                    if (!std::isfinite(mass) || mass <= 0)
+                        return fail(QM_E_MASS, "The state has no finite positive probability mass.");
+                }
+                const int p = rot[(size_t)r].parameter;
+                for (int t = 0; t < term_count; ++t) {
+                    double plus, minus;
+                    if (!value(cp, t, plus) || !value(cm, t, minus))
+                        return fail(QM_E_MASS, "The observable accumulation is nonfinite.");
+                    const double contribution = coef(v, t) * (0.5 * plus - 0.5 * minus);
+                    neumaier_add(grad[p], correction[(size_t)p], contribution);
+                    if (!std::isfinite(grad[p]) || !std::isfinite(correction[(size_t)p]))
+                        return fail(QM_E_MASS, "The gradient accumulation is nonfinite.");
+                }
+            }
+            for (int p = 0; p < parameter_count; ++p) {
+                grad[p] += correction[(size_t)p];
+                if (!std::isfinite(grad[p])) return fail(QM_E_MASS, "The gradient is nonfinite.");
+            }
+        }
+        return QM_OK;
+    }
+};
+
+// Runs problems of any sizes together.  The device budget is shared in proportion to each
+// problem's state bytes; in every round each problem runs its next wave, on its own stream when
+// there are several (forked from and joined to the context's stream), so the sizes overlap on
+// the device.  Rounds in which every problem runs a full wave replay a captured CUDA graph (one
+// per host buffer): a single launch covers all sizes of the round.
+int32_t run_problems(qm_context* ctx, std::vector<std::unique_ptr<VqeProblem>>& problems, qm_vqe_stats* stats) {
+    auto wall0 = std::chrono::steady_clock::now();
+    if (!ctx) return fail(QM_E_ARG, "context is null");
+    for (auto& p : problems) {
+        int32_t rc = p->validate();
+        if (rc) return rc;
+    }
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    if (ctx->disposed) return fail(QM_E_DISPOSED, "context disposed");
+    QM_CUDA(cudaSetDevice(ctx->device));
+    for (auto& p : problems) {
+        int32_t rc = p->prepare(ctx);
+        if (rc) return rc;
+    }
+    const int64_t free_budget = ctx->device_budget - ctx->device_in_use;
+    double total_work = 0;
+    for (auto& p : problems) total_work += (double)p->circuits * (double)p->state_bytes();
+    for (auto& p : problems) {
+        const int64_t share = problems.size() == 1
+                                  ? free_budget
+                                  : (int64_t)((double)free_budget * ((double)p->circuits * p->state_bytes() / total_work));
+        int32_t rc = p->allocate(ctx, share);
+        if (rc) return rc;
+    }
+    const bool multi = problems.size() > 1;
+    cudaStream_t main = ctx->stream;
+    for (auto& p : problems) {
+        if (multi) {
+            QM_CUDA(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+            p->own_stream = true;
+        } else {
+            p->stream = main;
+        }
+    }
+    std::vector<cudaEvent_t> events;
+    struct EventGuard {
+        std::vector<cudaEvent_t>& e;
+        ~EventGuard() {
+            for (cudaEvent_t x : e) cudaEventDestroy(x);
+        }
+    } eg{events};
+    auto make_event = [&](unsigned flags, cudaEvent_t* out) -> int32_t {
+        QM_CUDA(cudaEventCreateWithFlags(out, flags));
+        events.push_back(*out);
+        return QM_OK;
+    };
+    cudaEvent_t done[2], e0, e1, fork;
+    std::vector<cudaEvent_t> join(problems.size());
+    int32_t rc = make_event(cudaEventDisableTiming, &done[0]);
+    if (!rc) rc = make_event(cudaEventDisableTiming, &done[1]);
+    if (!rc) rc = make_event(cudaEventDefault, &e0);
+    if (!rc) rc = make_event(cudaEventDefault, &e1);
+    if (!rc) rc = make_event(cudaEventDisableTiming, &fork);
+    for (size_t i = 0; !rc && i < problems.size(); ++i) rc = make_event(cudaEventDisableTiming, &join[i]);
+    if (rc) return rc;
+
+    int64_t rounds = 0;
+    for (auto& p : problems) rounds = std::max(rounds, p->waves());
+    // one round: every active problem's wave, forked from and joined to the context's stream
+    auto enqueue_round = [&](int buf, int64_t r) -> int32_t {
+        if (multi) QM_CUDA(cudaEventRecord(fork, main));
+        for (size_t i = 0; i < problems.size(); ++i) {
+            VqeProblem& p = *problems[i];
+            if (r >= p.waves()) continue;
+            const int count = (int)std::min<int64_t>(p.B, p.circuits - r * p.B);
+            if (multi) QM_CUDA(cudaStreamWaitEvent(p.stream, fork, 0));
+            int32_t r2 = p.enqueue_wave(buf, count, p.stream);
+            if (r2) return r2;
+            if (multi) {
+                QM_CUDA(cudaEventRecord(join[i], p.stream));
+                QM_CUDA(cudaStreamWaitEvent(main, join[i], 0));
+            }
+        }
+        return QM_OK;
+    };
+    auto full_round = [&](int64_t r) {
+        for (auto& p : problems)
+            if (r >= p->waves() || (r + 1) * p->B > p->circuits) return false;
+        return true;
+    };
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     struct GraphGuard {
         cudaGraphExec_t* g;
@@ -590,131 +757,117 @@ int32_t vqe_evaluate(qm_context* ctx, int32_t qubits, int32_t precision, const q
                 if (g[i]) cudaGraphExecDestroy(g[i]);
         }
     } gg{graph};
-    const bool use_graphs = waves >= 3;
-    QM_CUDA(cudaEventRecord(e0, st));
-    int64_t pending_first[2] = {-1, -1};
-    int pending_count[2] = {0, 0};
+    const bool use_graphs = rounds >= 3;
+    QM_CUDA(cudaEventRecord(e0, main));
+    bool pending[2] = {false, false};
     auto collect = [&](int buf) -> int32_t {
-        if (pending_first[buf] < 0) return QM_OK;
+        if (!pending[buf]) return QM_OK;
         QM_CUDA(cudaEventSynchronize(done[buf]));
-        std::memcpy(&results[(size_t)pending_first[buf] * tp.columns], h_out[buf],
-                    sizeof(double) * (size_t)pending_count[buf] * tp.columns);
-        pending_first[buf] = -1;
+        for (auto& p : problems) p->collect(buf);
+        pending[buf] = false;
         return QM_OK;
     };
-    for (int64_t w = 0; w < waves; ++w) {
-        const int buf = (int)(w & 1);
-        rc = collect(buf);  // the host buffer is free again
+    for (int64_t r = 0; r < rounds; ++r) {
+        const int buf = (int)(r & 1);
+        rc = collect(buf);  // the host buffers of this parity are free again
         if (rc) return rc;
-        const int64_t first = w * B;
-        const int count = (int)std::min<int64_t>(B, circuits - first);
-        fill_table(h_table[buf], first, count);
-        if (use_graphs && count == B) {
-            if (!graph[buf]) {
-                if (w < 2) {
-                    // first use of this buffer runs eagerly (configures kernel attributes), then captures
-                    rc = enqueue_wave(buf, count);
-                    if (rc) return rc;
-                    QM_CUDA(cudaEventRecord(done[buf], st));
-                    pending_first[buf] = first;
-                    pending_count[buf] = count;
-                    cudaGraph_t g;
-                    QM_CUDA(cudaStreamSynchronize(st));
-                    QM_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-                    int32_t r3 = enqueue_wave(buf, count);
-                    cudaError_t ce = cudaStreamEndCapture(st, &g);
-                    if (r3) return r3;
-                    if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
-                    ce = cudaGraphInstantiate(&graph[buf], g, 0);
-                    cudaGraphDestroy(g);
-                    if (ce != cudaSuccess) return cuda_fail(ce, "cudaGraphInstantiate");
-                    continue;
+        for (auto& p : problems) {
+            if (r >= p->waves()) continue;
+            const int64_t first = r * p->B;
+            const int count = (int)std::min<int64_t>(p->B, p->circuits - first);
+            p->fill_table(buf, first, count);
+            p->pending_first[buf] = first;
+            p->pending_count[buf] = count;
+        }
+        if (use_graphs && full_round(r)) {
+            if (!graph[buf] && r < 2) {
+                // first use of this buffer runs eagerly (configures kernel attributes), then captures
+                rc = enqueue_round(buf, r);
+                if (rc) {
+                    cudaStreamSynchronize(main);
+                    return rc;
+                }
+                QM_CUDA(cudaEventRecord(done[buf], main));
+                pending[buf] = true;
+                cudaGraph_t g;
+                QM_CUDA(cudaStreamSynchronize(main));
+                QM_CUDA(cudaStreamBeginCapture(main, cudaStreamCaptureModeThreadLocal));
+                int32_t r3 = enqueue_round(buf, r);
+                cudaError_t ce = cudaStreamEndCapture(main, &g);
+                if (r3) return r3;
+                if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
+                ce = cudaGraphInstantiate(&graph[buf], g, 0);
+                cudaGraphDestroy(g);
+                if (ce != cudaSuccess) return cuda_fail(ce, "cudaGraphInstantiate");
+                continue;
+            }
+            if (graph[buf]) {
+                QM_CUDA(cudaGraphLaunch(graph[buf], main));
+            } else {
+                rc = enqueue_round(buf, r);
+                if (rc) {
+                    cudaStreamSynchronize(main);
+                    return rc;
                 }
             }
-            QM_CUDA(cudaGraphLaunch(graph[buf], st));
         } else {
-            rc = enqueue_wave(buf, count);
+            rc = enqueue_round(buf, r);
             if (rc) {
-                cudaStreamSynchronize(st);
+                cudaStreamSynchronize(main);
                 return rc;
             }
         }
-        QM_CUDA(cudaEventRecord(done[buf], st));
-        pending_first[buf] = first;
-        pending_count[buf] = count;
+        QM_CUDA(cudaEventRecord(done[buf], main));
+        pending[buf] = true;
     }
     rc = collect(0);
     if (rc) return rc;
     rc = collect(1);
     if (rc) return rc;
-    QM_CUDA(cudaEventRecord(e1, st));
-    QM_CUDA(cudaStreamSynchronize(st));
+    QM_CUDA(cudaEventRecord(e1, main));
+    QM_CUDA(cudaStreamSynchronize(main));
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
-
-    // assembly in the reference's order (StateVector.Energy.cs:22-45,
-    // VariationalEnergyEvaluator.cs:45-85)
-    auto value = [&](int64_t c, int t, double& out) -> bool {
-        const double mass = results[(size_t)c * tp.columns + tp.mass_column];
-        const double raw = results[(size_t)c * tp.columns + t];
-        if (!std::isfinite(mass) || mass <= 0 || !std::isfinite(raw)) return false;
-        out = raw / mass;
-        return true;
-    };
-    for (int v = 0; v < vectors; ++v) {
-        const int64_t c0 = (int64_t)v * per_vector;
-        {
-            const double mass = results[(size_t)c0 * tp.columns + tp.mass_column];
-            if (!std::isfinite(mass) || mass <= 0) return fail(QM_E_MASS, "The state has no finite positive probability mass.");
-        }
-        double sum = 0, corr = 0;
-        for (int t = 0; t < term_count; ++t) {
-            const double ct = coef(v, t);
-            if (ct == 0) continue;
-            double e;
-            if (!value(c0, t, e)) return fail(QM_E_MASS, "The observable accumulation is nonfinite.");
-            neumaier_add(sum, corr, ct * e);
-            if (!std::isfinite(sum) || !std::isfinite(corr)) return fail(QM_E_MASS, "The energy accumulation is nonfinite.");
-        }
-        const double energy = sum + corr;
-        if (!std::isfinite(energy)) return fail(QM_E_MASS, "The energy is nonfinite.");
-        energies[v] = energy;
-        if (!with_gradient) continue;
-        double* grad = gradients + (size_t)v * parameter_count;
-        std::vector<double> correction((size_t)parameter_count, 0.0);
-        for (int p = 0; p < parameter_count; ++p) grad[p] = 0.0;
-        for (int r = 0; r < R; ++r) {
-            const int64_t cp = c0 + 1 + 2 * r, cm = cp + 1;
-            for (int64_t c : {cp, cm}) {
-                const double mass = results[(size_t)c * tp.columns + tp.mass_column];
-                if (!std::isfinite(mass) || mass <= 0) return fail(QM_E_MASS, "The state has no finite positive probability mass.");
-            }
-            const int p = rot[(size_t)r].parameter;
-            for (int t = 0; t < term_count; ++t) {
-                double plus, minus;
-                if (!value(cp, t, plus) || !value(cm, t, minus)) return fail(QM_E_MASS, "The observable accumulation is nonfinite.");
-                const double contribution = coef(v, t) * (0.5 * plus - 0.5 * minus);
-                neumaier_add(grad[p], correction[(size_t)p], contribution);
-                if (!std::isfinite(grad[p]) || !std::isfinite(correction[(size_t)p]))
-                    return fail(QM_E_MASS, "The gradient accumulation is nonfinite.");
-            }
-        }
-        for (int p = 0; p < parameter_count; ++p) {
-            grad[p] += correction[(size_t)p];
-            if (!std::isfinite(grad[p])) return fail(QM_E_MASS, "The gradient is nonfinite.");
-        }
+    for (auto& p : problems) {
+        rc = p->assemble();
+        if (rc) return rc;
     }
     if (stats) {
         std::memset(stats, 0, sizeof *stats);
-        stats->circuits = circuits;
-        stats->waves = (int32_t)waves;
-        stats->batch_states = B;
-        stats->passes_per_circuit = (int32_t)plan.passes.size();
-        stats->tile_passes = (int32_t)tp.passes.size();
+        for (auto& p : problems) {
+            stats->circuits += p->circuits;
+            stats->batch_states += p->B;
+            stats->passes_per_circuit = std::max(stats->passes_per_circuit, (int32_t)p->plan.passes.size());
+            stats->tile_passes = std::max(stats->tile_passes, (int32_t)p->tp.passes.size());
+        }
+        stats->waves = (int32_t)rounds;
         stats->device_seconds = ms * 1e-3;
         stats->wall_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - wall0).count();
     }
     return QM_OK;
+}
+
+int32_t vqe_evaluate(qm_context* ctx, int32_t qubits, int32_t precision, const qm_template_op* ops, int32_t op_count,
+                     int32_t parameter_count, const qm_pauli_term* terms, int32_t term_count, const double* coefficients,
+                     const double* parameters, int32_t vectors, int32_t with_gradient, double* energies,
+                     double* gradients, qm_vqe_stats* stats) {
+    std::vector<std::unique_ptr<VqeProblem>> problems;
+    problems.emplace_back(new VqeProblem());
+    VqeProblem& p = *problems[0];
+    p.qubits = qubits;
+    p.precision = precision;
+    p.ops = ops;
+    p.op_count = op_count;
+    p.parameter_count = parameter_count;
+    p.terms = terms;
+    p.term_count = term_count;
+    p.coefficients = coefficients;
+    p.parameters = parameters;
+    p.vectors = vectors;
+    p.with_gradient = with_gradient;
+    p.energies = energies;
+    p.gradients = gradients;
+    return run_problems(ctx, problems, stats);
 }
 
 }  // namespace
@@ -736,4 +889,31 @@ extern "C" int32_t qm_vqe_evaluate_coefficients(qm_context* ctx, int32_t qubits,
     if (term_count > 0 && !coefficients) return fail(QM_E_ARG, "coefficients is null");
     return vqe_evaluate(ctx, qubits, precision, ops, op_count, parameter_count, terms, term_count, coefficients,
                         parameters, vectors, with_gradient, energies, gradients, stats);
+}
+
+static_assert(sizeof(qm_vqe_problem) == 80, "qm_vqe_problem layout");
+
+extern "C" int32_t qm_vqe_evaluate_mixed(qm_context* ctx, const qm_vqe_problem* list, int32_t count,
+                                         qm_vqe_stats* stats) {
+    if (count < 1 || !list) return fail(QM_E_ARG, "problems");
+    std::vector<std::unique_ptr<VqeProblem>> problems;
+    for (int32_t i = 0; i < count; ++i) {
+        const qm_vqe_problem& q = list[i];
+        problems.emplace_back(new VqeProblem());
+        VqeProblem& p = *problems.back();
+        p.qubits = q.qubits;
+        p.precision = q.precision;
+        p.ops = q.operations;
+        p.op_count = q.operation_count;
+        p.parameter_count = q.parameter_count;
+        p.terms = q.terms;
+        p.term_count = q.term_count;
+        p.coefficients = q.coefficients;
+        p.parameters = q.parameters;
+        p.vectors = q.vectors;
+        p.with_gradient = q.with_gradient;
+        p.energies = q.energies;
+        p.gradients = q.gradients;
+    }
+    return run_problems(ctx, problems, stats);
 }

@@ -32,6 +32,9 @@
 #include "qm_internal.h"
 #include "qm_serve_policy.h"
 
+static_assert(sizeof(qm_serve_options) == 56 && sizeof(qm_serve_result) == 72 && sizeof(qm_serve_stats) == 80,
+              "serving ABI sizes");
+
 namespace {
 
 using Clock = std::chrono::steady_clock;

@@ -203,6 +203,38 @@ class B200VariationalEnergyEvaluator:
                                stats.batch_states, stats.passes_per_circuit, stats.tile_passes, stats.device_seconds,
                                stats.wall_seconds)
 
+    def EvaluateMixed(self, problems: Sequence[tuple], withGradient: bool = True) -> tuple[list, BatchEvaluation]:
+        """Several (circuit, hamiltonian, parameters) problems of different sizes in one call
+        (qm_vqe_evaluate_mixed): each round of waves covers every size, as one CUDA graph launch
+        once the rounds are full.  Returns each problem's (energies, gradients) and the totals."""
+        keep, recs, outs = [], (_lib.VqeProblem * len(problems))(), []
+        for i, (circuit, hamiltonian, parameters) in enumerate(problems):
+            self._validate(circuit, hamiltonian)
+            params = np.ascontiguousarray(parameters, dtype=np.float64)
+            if params.ndim == 1:
+                params = params.reshape(1, -1)
+            vectors, pcount = params.shape
+            if pcount != circuit.ParameterCount:
+                raise ArgumentError("Binding size must match ParameterCount.")
+            ops, nops = circuit.template_array()
+            terms, nterms = terms_array(hamiltonian.Terms)
+            energies = np.zeros(vectors, dtype=np.float64)
+            grads = np.zeros((vectors, max(1, pcount)), dtype=np.float64)
+            keep += [ops, terms, params, energies, grads]
+            r = recs[i]
+            r.qubits, r.precision, r.operations, r.operation_count = circuit.QubitCount, self.precision, \
+                C.cast(ops, C.c_void_p), nops
+            r.parameter_count, r.terms, r.term_count, r.vectors = pcount, C.cast(terms, C.c_void_p), nterms, vectors
+            r.coefficients, r.parameters = None, params.ctypes.data_as(_lib.DP)
+            r.with_gradient, r.energies, r.gradients = 1 if withGradient else 0, energies.ctypes.data_as(_lib.DP), \
+                grads.ctypes.data_as(_lib.DP)
+            outs.append((energies, grads[:, :pcount] if withGradient else None))
+        stats = _lib.VqeStats()
+        check(load().qm_vqe_evaluate_mixed(self.context.handle, recs, len(problems), C.byref(stats)))
+        total = BatchEvaluation(None, None, stats.circuits, stats.waves, stats.batch_states, stats.passes_per_circuit,
+                                stats.tile_passes, stats.device_seconds, stats.wall_seconds)
+        return outs, total
+
     def Evaluate(self, circuit: ParameterizedCircuit, hamiltonian: PauliHamiltonian,
                  parameters: Sequence[float]) -> float:
         circuit._check(parameters)

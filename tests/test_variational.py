@@ -223,3 +223,29 @@ def test_compiled_tile_expectation_matches_the_oracle(gpu_context, diagonal, fp3
     for v in range(3):
         want = ref.energy(c, h, params[v])
         assert abs(got.Energies[v] - want) <= (1e-6 if fp32 else 5e-12) * scale, (v, got.Energies[v], want)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("fp32", [False, True])
+def test_mixed_sizes_equal_separate_evaluations(gpu_context, fp32):
+    """qm_vqe_evaluate_mixed: 10-, 12- and 14-qubit problems together (their own streams, rounds
+    replayed as one graph) give the separate calls' energies and gradients bit for bit."""
+    from quantummatter_b200.backend import FP32, FP64, B200BackendOptions, B200Context
+    from quantummatter_b200.variational import B200VariationalEnergyEvaluator
+    # a small device budget: several waves per size, so full rounds replay the captured graph
+    ctx = B200Context(B200BackendOptions(DeviceMemoryBudgetBytes=48 << 20, StagingMemoryBudgetBytes=1 << 30))
+    ev = B200VariationalEnergyEvaluator(ctx, FP32 if fp32 else FP64)
+    problems = []
+    for n in (10, 12, 14):
+        c = hardware_efficient_ansatz(n, 2)
+        problems.append((c, xxz_chain(n, seed=n), uniform_parameters(c.ParameterCount, 3, -math.pi, math.pi, seed=n)))
+    try:
+        outs, total = ev.EvaluateMixed(problems)
+        assert total.Circuits == sum(3 * (1 + 2 * len(c.RotationParameterIndices)) for c, _, _ in problems)
+        assert total.Waves >= 3
+        for (c, h, p), (e, g) in zip(problems, outs):
+            alone = B200VariationalEnergyEvaluator(gpu_context, ev.precision).EvaluateBatch(c, h, p, withGradient=True)
+            assert np.array_equal(e, alone.Energies)
+            assert np.array_equal(g, alone.Gradients)
+    finally:
+        ctx.Dispose()
