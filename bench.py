@@ -919,8 +919,20 @@ def main() -> None:
     fp64 = fp64_roofline(fp64_flops, args.steps, total, launches, clocks.summary())
     side32 = side_vqe = None
     if rank == 0 and world == 1 and precision == FP64 and args.circuit == "brick" and not args.no_side_runs:
-        side32 = fp32_side_run(ctx, circuit, state, plan, steps=3)
-        side_vqe = vqe_side_run(ctx)
+        # side runs never take the headline line down: a failure is reported in its place
+        try:
+            side32 = fp32_side_run(ctx, circuit, state, plan, steps=3)
+        except Exception as e:  # noqa: BLE001
+            side32 = {"error": f"{type(e).__name__}: {e}"}
+        try:
+            side_ctx = B200Context(B200BackendOptions(DeviceIndex=local, DeviceMemoryBudgetBytes=40 << 30,
+                                                      StagingMemoryBudgetBytes=1 << 30))
+            try:
+                side_vqe = vqe_side_run(side_ctx)
+            finally:
+                side_ctx.Dispose()
+        except Exception as e:  # noqa: BLE001
+            side_vqe = {"error": f"{type(e).__name__}: {e}"}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         state.Dispose()

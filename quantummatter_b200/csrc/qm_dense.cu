@@ -164,6 +164,9 @@ __global__ void __launch_bounds__(kDenseThreads, 1)
             if ((b >> i) & 1) w += tile_weight(P, P.q_bits[i]);
         wq[b] = w;
     }
+    int wbit[M];
+#pragma unroll
+    for (int q = 0; q < M; ++q) wbit[q] = tile_weight(P, P.q_bits[q]);
     int wl[RC];
 #pragma unroll
     for (int i = 0; i < RC; ++i) {
@@ -212,12 +215,19 @@ __global__ void __launch_bounds__(kDenseThreads, 1)
         for (int r = 0; r < RA; ++r)
 #pragma unroll
             for (int c = 0; c < RC; ++c) ar[r][c] = ai[r][c] = (T)0;
-#pragma unroll(D < 8 ? D : 8)
+        const V* col[RC];
+#pragma unroll
+        for (int c = 0; c < RC; ++c) col[c] = tile + wl[c];
+#pragma unroll
         for (int b = 0; b < D; ++b) {
-            const int off = wq[b];
+            // row b's offset: the sum of its fused bits' weights (b is a constant after unrolling)
+            int off = 0;
+#pragma unroll
+            for (int q = 0; q < M; ++q)
+                if ((b >> q) & 1) off += wbit[q];
             V x[RC], u[RA];
 #pragma unroll
-            for (int c = 0; c < RC; ++c) x[c] = tile[off + wl[c]];
+            for (int c = 0; c < RC; ++c) x[c] = col[c][off];
 #pragma unroll
             for (int r = 0; r < RA; ++r) u[r] = U[b * D + rg * RA + r];
 #pragma unroll

@@ -412,7 +412,7 @@ bool dense_tc_supported(int qubits, int precision, const DenseOp& op) {
 bool dense_tc_enabled() {
     static const bool on = [] {
         const char* e = std::getenv("QM_DENSE_TC");
-        return !(e && e[0] == '0');
+        return e && e[0] == '1';
     }();
     return on;
 }

@@ -186,7 +186,7 @@ bool dense_geometry(int qubits, int precision, const DenseOp& op, DenseGeometry&
 cudaError_t launch_dense(void* amps, int qubits, int precision, const DenseOp& op, const double2* matrix,
                          int32_t* status, int sm_count, cudaStream_t s);
 // 6-qubit fused gates on complex64 states of at least 11 qubits run on the tensor cores
-// (qm_dense_tc.cu, 3xTF32); QM_DENSE_TC=0 keeps them on the FP32 pipes.
+// (qm_dense_tc.cu, 3xTF32) when QM_DENSE_TC=1; otherwise they stay on the FP32 pipes.
 bool dense_tc_enabled();
 bool dense_tc_supported(int qubits, int precision, const DenseOp& op);
 void dense_tc_image(const double* transposed_unitary, std::vector<float>& image);

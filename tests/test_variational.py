@@ -233,7 +233,8 @@ def test_mixed_sizes_equal_separate_evaluations(gpu_context, fp32):
     from quantummatter_b200.backend import FP32, FP64, B200BackendOptions, B200Context
     from quantummatter_b200.variational import B200VariationalEnergyEvaluator
     # a small device budget: several waves per size, so full rounds replay the captured graph
-    ctx = B200Context(B200BackendOptions(DeviceMemoryBudgetBytes=48 << 20, StagingMemoryBudgetBytes=1 << 30))
+    ctx = B200Context(B200BackendOptions(DeviceMemoryBudgetBytes=(24 if fp32 else 48) << 20,
+                                         StagingMemoryBudgetBytes=1 << 30))
     ev = B200VariationalEnergyEvaluator(ctx, FP32 if fp32 else FP64)
     problems = []
     for n in (10, 12, 14):
