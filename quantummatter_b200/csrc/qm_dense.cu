@@ -20,9 +20,11 @@
 // Every wait on an mbarrier is bounded (about a second of clock cycles); a wait that runs out
 // records QM_E_TIMEOUT in the launch's status word and the CTA waits, again bounded, for its own
 // copies in flight before it returns.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <mutex>
 
 #include "qm_device.cuh"
@@ -38,7 +40,15 @@ constexpr int kDenseMaxBufs = 4;
 constexpr long long kWaitCycles = 2000000000ll;  // about one second at the B200's clocks
 constexpr int kDenseSmemMax = 226 * 1024;        // dynamic shared memory; the static part stays below 1 KiB
 
+constexpr int kTmaMaxRank = 5;
+
 struct DenseLaunch {
+    // Tensor-map path: the tile is one box of a tensor map over the state whose dimensions are the
+    // runs of tile and outer index bits from bit 0 up (tile runs: full extent in the box; outer
+    // runs: extent 1, coordinate from the work item); one cp.async.bulk.tensor moves the tile.
+    CUtensorMap tmap;
+    int32_t tma_rank;         // 0: bulk copies of runs instead
+    int32_t tma_lo[kTmaMaxRank], tma_len[kTmaMaxRank], tma_tile[kTmaMaxRank];
     const double2* matrix;    // transposed unitary: row b holds U(a, b) for a = 0 .. 2^m-1
     int32_t* status;          // QM_E_TIMEOUT after a wait that ran out
     uint64_t items;           // tiles
@@ -46,10 +56,16 @@ struct DenseLaunch {
     uint32_t copy_mask;       // tile bits above the run, enumerated by the copy index
     int32_t q_bits[kDenseMaxQubits];
     int32_t l_bits[kDenseTileBits];
+    int32_t m;                // fused qubits
     int32_t cols_bits;        // c: column bits of the tile
-    int32_t run_bits;         // r: a copy moves the run of global bits [0, r)
-    int32_t copies;           // 2^(12 - r)
-    int32_t stride;           // elements between consecutive copies in shared memory
+    int32_t run_bits;         // r: the layout's runs are global bits [0, r)
+    int32_t copies;           // 2^(12 - r) runs per tile
+    int32_t stride;           // elements between consecutive runs in shared memory
+    // The bulk copies: runs of global bits [0, xfer_bits), one per value of the tile bits in
+    // xfer_mask, xfer_stride elements apart.  Unpadded layouts (runs under 128 bytes) are the tile's
+    // natural index order, so their copies take the longest natural runs instead.
+    uint32_t xfer_mask;
+    int32_t xfer_bits, xfers, xfer_stride, xfer_pad;
     int32_t nbuf;             // buffers in the ring
     int32_t buf_elems;        // elements per buffer
     int32_t buf_offset;       // byte offset of the first buffer in dynamic shared memory
@@ -105,23 +121,102 @@ __device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.w
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
+// coordinates of a work item's box: 0 on tile dimensions, the item's outer bits on the others
+__device__ __forceinline__ void tma_coords(const DenseLaunch& P, uint32_t base, int32_t (&c)[kTmaMaxRank]) {
+#pragma unroll
+    for (int d = 0; d < kTmaMaxRank; ++d)
+        c[d] = (d < P.tma_rank && !P.tma_tile[d]) ? (int32_t)((base >> P.tma_lo[d]) & ((1u << P.tma_len[d]) - 1u)) : 0;
+}
+
+__device__ __forceinline__ void tma_load(const DenseLaunch& P, void* dst, uint64_t* bar, const int32_t (&c)[kTmaMaxRank]) {
+    const uint64_t map = reinterpret_cast<uint64_t>(&P.tmap);
+    const uint32_t d = smem_u32(dst), b = smem_u32(bar);
+    switch (P.tma_rank) {
+    case 1:
+        asm volatile("cp.async.bulk.tensor.1d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2}], [%3];"
+                     ::"r"(d), "l"(map), "r"(c[0]), "r"(b) : "memory");
+        break;
+    case 2:
+        asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+                     ::"r"(d), "l"(map), "r"(c[0]), "r"(c[1]), "r"(b) : "memory");
+        break;
+    case 3:
+        asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+                     ::"r"(d), "l"(map), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(b) : "memory");
+        break;
+    case 4:
+        asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
+                     ::"r"(d), "l"(map), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(b) : "memory");
+        break;
+    default:
+        asm volatile("cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], [%7];"
+                     ::"r"(d), "l"(map), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(c[4]), "r"(b) : "memory");
+        break;
+    }
+}
+
+__device__ __forceinline__ void tma_store(const DenseLaunch& P, const void* src, const int32_t (&c)[kTmaMaxRank]) {
+    const uint64_t map = reinterpret_cast<uint64_t>(&P.tmap);
+    const uint32_t s = smem_u32(src);
+    switch (P.tma_rank) {
+    case 1:
+        asm volatile("cp.async.bulk.tensor.1d.global.shared::cta.bulk_group [%0, {%1}], [%2];" ::"l"(map), "r"(c[0]), "r"(s)
+                     : "memory");
+        break;
+    case 2:
+        asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(map), "r"(c[0]),
+                     "r"(c[1]), "r"(s) : "memory");
+        break;
+    case 3:
+        asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(map),
+                     "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(s) : "memory");
+        break;
+    case 4:
+        asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.bulk_group [%0, {%1, %2, %3, %4}], [%5];" ::"l"(map),
+                     "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(s) : "memory");
+        break;
+    default:
+        asm volatile("cp.async.bulk.tensor.5d.global.shared::cta.bulk_group [%0, {%1, %2, %3, %4, %5}], [%6];" ::"l"(map),
+                     "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(c[4]), "r"(s) : "memory");
+        break;
+    }
+}
+
 template <typename V>
 __device__ __forceinline__ void issue_tile_load(const DenseLaunch& P, const V* s, V* buf, uint64_t* bar,
                                                 uint64_t item, int lane) {
     const uint32_t base = deposit((uint32_t)item, P.outer_mask);
-    const uint32_t run_bytes = (uint32_t)sizeof(V) << P.run_bits;
-    if (lane == 0) mbar_arrive_expect_tx(bar, run_bytes * (uint32_t)P.copies);
+    if (P.tma_rank) {
+        if (lane == 0) {
+            int32_t c[kTmaMaxRank];
+            tma_coords(P, base, c);
+            mbar_arrive_expect_tx(bar, (uint32_t)sizeof(V) << (P.cols_bits + P.m));
+            tma_load(P, buf, bar, c);
+        }
+        return;
+    }
+    const uint32_t run_bytes = (uint32_t)sizeof(V) << P.xfer_bits;
+    if (lane == 0) mbar_arrive_expect_tx(bar, run_bytes * (uint32_t)P.xfers);
     __syncwarp();
-    for (int x = lane; x < P.copies; x += 32)
-        bulk_load(buf + (size_t)x * P.stride, s + (base | deposit((uint32_t)x, P.copy_mask)), run_bytes, bar);
+    for (int x = lane; x < P.xfers; x += 32)
+        bulk_load(buf + (size_t)x * P.xfer_stride, s + (base | deposit((uint32_t)x, P.xfer_mask)), run_bytes, bar);
 }
 
 template <typename V>
 __device__ __forceinline__ void issue_tile_store(const DenseLaunch& P, V* s, const V* buf, uint64_t item, int lane) {
     const uint32_t base = deposit((uint32_t)item, P.outer_mask);
-    const uint32_t run_bytes = (uint32_t)sizeof(V) << P.run_bits;
-    for (int x = lane; x < P.copies; x += 32)
-        bulk_store(s + (base | deposit((uint32_t)x, P.copy_mask)), buf + (size_t)x * P.stride, run_bytes);
+    if (P.tma_rank) {
+        if (lane == 0) {
+            int32_t c[kTmaMaxRank];
+            tma_coords(P, base, c);
+            tma_store(P, buf, c);
+            bulk_commit();
+        }
+        return;
+    }
+    const uint32_t run_bytes = (uint32_t)sizeof(V) << P.xfer_bits;
+    for (int x = lane; x < P.xfers; x += 32)
+        bulk_store(s + (base | deposit((uint32_t)x, P.xfer_mask)), buf + (size_t)x * P.xfer_stride, run_bytes);
     bulk_commit();
 }
 
@@ -327,7 +422,32 @@ cudaError_t launch_dense_t(void* amps, int m, const DenseLaunch& P, int grid, in
     }
 }
 
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// cuTensorMapEncodeTiled from the driver, through the runtime (the library does not link libcuda)
+EncodeTiled tensor_map_encoder() {
+    static const EncodeTiled fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return (EncodeTiled) nullptr;
+        return reinterpret_cast<EncodeTiled>(p);
+    }();
+    return fn;
+}
+
 }  // namespace
+
+bool dense_tma_enabled() {
+    static const bool on = [] {
+        const char* e = std::getenv("QM_DENSE_TMA");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
 
 bool dense_geometry(int qubits, int precision, const DenseOp& op, DenseGeometry& g) {
     const int m = op.m;
@@ -360,8 +480,47 @@ bool dense_geometry(int qubits, int precision, const DenseOp& op, DenseGeometry&
     g.copy_mask = (qmask | lmask) & ~((1u << r) - 1u);
     g.copies = 1 << (tb - r);
     const int run_bytes = elem << r;
-    const int pad = run_bytes >= 128 ? 16 / elem : 0;
+    // tensor-map dimensions: runs of tile / outer bits from bit 0 up; a tile run is split into
+    // boxes of at most 2^7 elements for the innermost dimension (256 scalars) and 2^8 otherwise
+    g.tma_rank = 0;
+    {
+        const uint32_t tile = qmask | lmask;
+        int rank = 0, b = 0;
+        bool ok = true;
+        while (b < qubits && ok) {
+            const bool in = (tile >> b) & 1u;
+            int len = 0;
+            while (b + len < qubits && (((tile >> (b + len)) & 1u) != 0) == in) ++len;
+            int lo = b;
+            while (len > 0) {
+                const int cap = in ? (rank == 0 ? 7 : 8) : 32;
+                const int l = std::min(len, cap);
+                if (rank == kDenseTmaMaxRank) {
+                    ok = false;
+                    break;
+                }
+                g.tma_lo[rank] = lo;
+                g.tma_len[rank] = l;
+                g.tma_tile[rank] = in ? 1 : 0;
+                ++rank;
+                lo += l;
+                len -= l;
+            }
+            b = lo;
+        }
+        if (ok && dense_tma_enabled()) g.tma_rank = rank;
+    }
+    // padding keeps column accesses free of bank conflicts, but a tensor-map box is unpadded
+    const int pad = (run_bytes >= 128 && g.tma_rank == 0) ? 16 / elem : 0;
     g.stride = (1 << r) + pad;
+    // copies: the layout's runs when padded, else the longest natural runs of the tile
+    int rn = r;
+    if (pad == 0)
+        while (rn < qubits && rn < 31 && ((qmask | lmask) >> rn & 1u)) ++rn;
+    g.xfer_bits = rn;
+    g.xfer_mask = (qmask | lmask) & ~((1u << rn) - 1u);
+    g.xfers = 1 << (tb - rn);
+    g.xfer_stride = pad == 0 ? (1 << rn) : g.stride;
     const int buf_bytes = ((g.copies * g.stride * elem + 127) / 128) * 128;
     g.buf_elems = buf_bytes / elem;
     const int header = ((elem * (1 << m) * (1 << m) + 4 * 64 + 8 * kDenseMaxBufs + 127) / 128) * 128;
@@ -400,6 +559,49 @@ cudaError_t launch_dense(void* amps, int qubits, int precision, const DenseOp& o
     P.run_bits = g.run_bits;
     P.copies = g.copies;
     P.stride = g.stride;
+    P.xfer_mask = g.xfer_mask;
+    P.xfer_bits = g.xfer_bits;
+    P.xfers = g.xfers;
+    P.xfer_stride = g.xfer_stride;
+    P.m = op.m;
+    P.tma_rank = 0;
+    if (g.tma_rank) {
+        auto encode = tensor_map_encoder();
+        if (encode) {
+            cuuint64_t dims[kTmaMaxRank], strides[kTmaMaxRank];
+            cuuint32_t box[kTmaMaxRank], estr[kTmaMaxRank];
+            const int elem = precision == QM_FP32 ? 8 : 16;
+            for (int d = 0; d < g.tma_rank; ++d) {
+                dims[d] = (cuuint64_t)1 << g.tma_len[d];
+                box[d] = g.tma_tile[d] ? (cuuint32_t)1 << g.tma_len[d] : 1u;
+                estr[d] = 1;
+                if (d > 0) strides[d - 1] = (cuuint64_t)elem << g.tma_lo[d];
+                P.tma_lo[d] = g.tma_lo[d];
+                P.tma_len[d] = g.tma_len[d];
+                P.tma_tile[d] = g.tma_tile[d];
+            }
+            dims[0] *= 2;  // the innermost dimension counts scalars: (re, im) pairs
+            box[0] *= 2;
+            const CUresult cr =
+                encode(&P.tmap, precision == QM_FP32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+                       (cuuint32_t)g.tma_rank, amps, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                       CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            if (cr == CUDA_SUCCESS) P.tma_rank = g.tma_rank;
+        }
+        if (!P.tma_rank) {
+            // no encoder: the unpadded layout's natural runs through bulk copies
+            P.xfer_bits = g.run_bits;
+            P.xfer_mask = g.copy_mask;
+            P.xfers = g.copies;
+            P.xfer_stride = g.stride;
+            int rn = g.run_bits;
+            while (rn < qubits && ((g.qmask | g.lmask) >> rn & 1u)) ++rn;
+            P.xfer_bits = rn;
+            P.xfer_mask = (g.qmask | g.lmask) & ~((1u << rn) - 1u);
+            P.xfers = 1 << (g.cols_bits + op.m - rn);
+            P.xfer_stride = 1 << rn;
+        }
+    }
     P.nbuf = g.nbuf;
     P.buf_elems = g.buf_elems;
     P.buf_offset = g.buf_offset;

@@ -130,6 +130,10 @@ struct DenseGeometry {
     uint32_t qmask, lmask, copy_mask, outer_mask;
     int32_t l_bits[12];
     int32_t cols_bits, run_bits, copies, stride, buf_elems, nbuf, buf_offset;
+    uint32_t xfer_mask;
+    int32_t xfer_bits, xfers, xfer_stride;
+    int32_t tma_rank;   // tensor-map dimensions of the tile's box, 0 when it needs more than five
+    int32_t tma_lo[5], tma_len[5], tma_tile[5];
     size_t smem;
     uint64_t items;
 };
@@ -182,6 +186,10 @@ int default_block_qubits(int qubits, int precision);
 bool plan_dense(const std::vector<qm_gate>& gates, int qubits, int precision, int width, Plan& plan,
                 std::string& error);
 bool dense_geometry(int qubits, int precision, const DenseOp& op, DenseGeometry& g);
+// Tiles of dense fused gates move as tensor-map boxes (cp.async.bulk.tensor) where their bit runs
+// form at most five dimensions; QM_DENSE_TMA=0 keeps them on plain bulk copies.
+constexpr int kDenseTmaMaxRank = 5;
+bool dense_tma_enabled();
 // One dense fused gate on a state (qm_dense.cu); `matrix` is its transposed unitary in device memory.
 cudaError_t launch_dense(void* amps, int qubits, int precision, const DenseOp& op, const double2* matrix,
                          int32_t* status, int sm_count, cudaStream_t s);
