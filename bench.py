@@ -57,13 +57,18 @@ def fp64_roofline(flops_per_step: float, steps: int, seconds: float, launches: i
             "flops_per_launch": flops_per_step / max(1, launches), "peak_source": "nominal at the sampled SM clock"}
 
 
-def profile_traffic(kernel_key: str) -> float | None:
-    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+def profile_value(name: str, kernel_key: str) -> float | None:
+    """A figure of the dominant kernel from the committed ncu summaries (`name[kernel]: value`)."""
     for f in sorted((ROOT / "profiles").glob("*.md")):
-        m = re.search(rf"traffic\[{re.escape(kernel_key)}\]:\s*([0-9.eE+]+)", f.read_text())
+        m = re.search(rf"{re.escape(name)}\[{re.escape(kernel_key)}\]:\s*([0-9.eE+]+)", f.read_text())
         if m:
             return float(m.group(1))
     return None
+
+
+def profile_traffic(kernel_key: str) -> float | None:
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary."""
+    return profile_value("traffic", kernel_key)
 
 
 class ClockSampler:
@@ -917,6 +922,11 @@ def main() -> None:
         backend.Dispose()
 
     fp64 = fp64_roofline(fp64_flops, args.steps, total, launches, clocks.summary())
+    counter = profile_value("fp64_pipe_active", kernel_key)
+    if counter is not None:
+        fp64["pipe_active_counter"] = counter
+        fp64["pipe_active_source"] = ("ncu sm__pipe_fp64_cycles_active of a 26-qubit capture of the same pass kind "
+                                      "(profiles/qm_pass_fp64_brick26q_full.md)")
     side32 = side_vqe = None
     if rank == 0 and world == 1 and precision == FP64 and args.circuit == "brick" and not args.no_side_runs:
         # side runs never take the headline line down: a failure is reported in its place
