@@ -16,7 +16,7 @@
 // Per CTA (one per SM), for a ring of tiles of 64 rows x 32 columns (2048 amplitudes, 16 KiB):
 //   - bulk copies (cp.async.bulk, mbarrier completion) stage each tile into one of four buffers,
 //     three tiles ahead of the one being converted;
-//   - all 256 threads split the tile into B_hi / B_lo in the canonical MN-major layout of the
+//   - all 256 threads split the tile into B_hi / B_lo in the canonical K-major layout of the
 //     MMA (two B buffers, so tile i converts while tile i-1's MMAs run);
 //   - one thread issues the 24 MMAs of the tile (8 K-steps x 3 products, M = 128, N = 64, K = 8)
 //     into one of two TMEM accumulators and commits them to an mbarrier;
@@ -50,8 +50,12 @@ constexpr size_t kTcSmemMax = 220 * 1024;
 
 // shared-memory layout (bytes)
 constexpr int kAHalf = 128 * 64 * 4;           // one 128 x 64 TF32 operand image: 32 KiB
-constexpr int kBSbo = 1040;                    // B: stride between groups of 4 real columns
-constexpr int kBHalf = (kTcN / 4) * kBSbo;     // one 64 x 64 B image: 16640 B
+// B, K-major without swizzle: core matrices of 8 real columns (n) x 4 rows (k, 16 bytes); the 16
+// k-groups of a column group 144 bytes apart (16 more than dense, so the conversion's stores of
+// k and k + 4 land in different banks), column groups 2304 bytes apart
+constexpr int kBLbo = 144;
+constexpr int kBSbo = 16 * kBLbo;              // 2304
+constexpr int kBHalf = (kTcN / 8) * kBSbo;     // one 64 x 64 B image: 18432 B
 constexpr int kOffA = 0;                       // A_hi, A_lo
 constexpr int kOffB = 2 * kAHalf;              // [2 buffers][hi, lo]
 constexpr int kOffStage = kOffB + 4 * kBHalf;  // staging ring, stage_bytes each
@@ -121,9 +125,9 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
     return d;
 }
 
-// Instruction descriptor of kind::tf32: FP32 accumulator, TF32 A (K-major) and B (MN-major),
-// M = 128, N = kTcN.
-constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | (1u << 16) | ((uint32_t)(kTcN >> 3) << 17) |
+// Instruction descriptor of kind::tf32: FP32 accumulator, TF32 A and B both K-major (an MN-major
+// TF32 operand without swizzle reads as zeros on B200), M = 128, N = kTcN.
+constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kTcN >> 3) << 17) |
                             ((uint32_t)(128 >> 4) << 24);
 
 __device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
@@ -257,7 +261,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_dense_tc(float2* __restrict__
         __syncthreads();
         if (abort_flag) break;
         if (i < tiles) {
-            // 3. split into the MMA's B layout: (k = b, n = 2j + c) at (n/4)*SBO + (b/8)*128 + (b%8)*16 + (n%4)*4
+            // 3. split into the MMA's B layout: (k = b, n = 2j + c) at (n%8)*16 + (n/8)*SBO + (b%4)*4 + (b/4)*LBO
             const float2* tile = stage + (size_t)cur * P.stage_elems;
             unsigned char* bhi = b_img + (size_t)bb * 2 * kBHalf;
             unsigned char* blo = bhi + kBHalf;
@@ -271,9 +275,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_dense_tc(float2* __restrict__
                 hi.y = tf32_head(x.y);
                 lo.x = x.x - hi.x;
                 lo.y = x.y - hi.y;
-                const int off = (j >> 1) * kBSbo + (b >> 3) * 128 + (b & 7) * 16 + (j & 1) * 8;
-                *reinterpret_cast<float2*>(bhi + off) = hi;
-                *reinterpret_cast<float2*>(blo + off) = lo;
+                const int n = 2 * j;  // real part in column n, imaginary part in column n + 1 (16 bytes on)
+                const int off = (n & 7) * 16 + (n >> 3) * kBSbo + (b & 3) * 4 + (b >> 2) * kBLbo;
+                *reinterpret_cast<float*>(bhi + off) = hi.x;
+                *reinterpret_cast<float*>(bhi + off + 16) = hi.y;
+                *reinterpret_cast<float*>(blo + off) = lo.x;
+                *reinterpret_cast<float*>(blo + off + 16) = lo.y;
             }
             fence_proxy_async();
         }
@@ -288,8 +295,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_dense_tc(float2* __restrict__
             for (int ks = 0; ks < 8; ++ks) {
                 const uint64_t ahi_d = smem_desc(a_base + ks * 256, 128, 2048);
                 const uint64_t alo_d = smem_desc(a_base + kAHalf + ks * 256, 128, 2048);
-                const uint64_t bhi_d = smem_desc(bhi + ks * 128, 128, kBSbo);
-                const uint64_t blo_d = smem_desc(blo + ks * 128, 128, kBSbo);
+                const uint64_t bhi_d = smem_desc(bhi + ks * 2 * kBLbo, kBLbo, kBSbo);
+                const uint64_t blo_d = smem_desc(blo + ks * 2 * kBLbo, kBLbo, kBSbo);
                 mma_tf32(d, ahi_d, bhi_d, ks > 0 ? 1u : 0u);
                 mma_tf32(d, ahi_d, blo_d, 1u);
                 mma_tf32(d, alo_d, bhi_d, 1u);
