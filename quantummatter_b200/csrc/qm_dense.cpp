@@ -169,14 +169,22 @@ bool plan_dense(const std::vector<qm_gate>& gates, int qubits, int precision, in
             plan.planned_bytes += 2 * touched * elem;
         } else {
             uint32_t mask = gr.mask;
-            // complex64 5-qubit gates join the tensor-core path as 6-qubit gates (U x I on the lowest
-            // free qubit): the extra multiply-adds are cheap there, the FP32 pipes are not
-            if (precision == QM_FP32 && popc(mask) == 5 && qubits >= 11 && dense_tc_enabled())
-                for (int q = 0; q < qubits; ++q)
-                    if (!(mask & (1u << q))) {
-                        mask |= 1u << q;
-                        break;
-                    }
+            // complex64 5-qubit gates join the tensor-core path as 6-qubit gates (U x I on one more
+            // qubit): the extra multiply-adds are cheap there, the FP32 pipes are not.  The qubit next
+            // to the group keeps its bits in one run (a scattered one would split the tile's copies).
+            if (precision == QM_FP32 && popc(mask) == 5 && qubits >= 11 && dense_tc_enabled()) {
+                const int top = 31 - __builtin_clz(mask), bottom = __builtin_ctz(mask);
+                if (top + 1 < qubits)
+                    mask |= 1u << (top + 1);
+                else if (bottom > 0)
+                    mask |= 1u << (bottom - 1);
+                else
+                    for (int q = 0; q < qubits; ++q)
+                        if (!(mask & (1u << q))) {
+                            mask |= 1u << q;
+                            break;
+                        }
+            }
             const int m = popc(mask);
             op.m = m;
             op.tc_image = -1;

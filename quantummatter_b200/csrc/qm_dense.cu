@@ -121,67 +121,6 @@ __device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.w
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
-// coordinates of a work item's box: 0 on tile dimensions, the item's outer bits on the others
-__device__ __forceinline__ void tma_coords(const DenseLaunch& P, uint32_t base, int32_t (&c)[kTmaMaxRank]) {
-#pragma unroll
-    for (int d = 0; d < kTmaMaxRank; ++d)
-        c[d] = (d < P.tma_rank && !P.tma_tile[d]) ? (int32_t)((base >> P.tma_lo[d]) & ((1u << P.tma_len[d]) - 1u)) : 0;
-}
-
-__device__ __forceinline__ void tma_load(const DenseLaunch& P, void* dst, uint64_t* bar, const int32_t (&c)[kTmaMaxRank]) {
-    const uint64_t map = reinterpret_cast<uint64_t>(&P.tmap);
-    const uint32_t d = smem_u32(dst), b = smem_u32(bar);
-    switch (P.tma_rank) {
-    case 1:
-        asm volatile("cp.async.bulk.tensor.1d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2}], [%3];"
-                     ::"r"(d), "l"(map), "r"(c[0]), "r"(b) : "memory");
-        break;
-    case 2:
-        asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
-                     ::"r"(d), "l"(map), "r"(c[0]), "r"(c[1]), "r"(b) : "memory");
-        break;
-    case 3:
-        asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
-                     ::"r"(d), "l"(map), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(b) : "memory");
-        break;
-    case 4:
-        asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
-                     ::"r"(d), "l"(map), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(b) : "memory");
-        break;
-    default:
-        asm volatile("cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], [%7];"
-                     ::"r"(d), "l"(map), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(c[4]), "r"(b) : "memory");
-        break;
-    }
-}
-
-__device__ __forceinline__ void tma_store(const DenseLaunch& P, const void* src, const int32_t (&c)[kTmaMaxRank]) {
-    const uint64_t map = reinterpret_cast<uint64_t>(&P.tmap);
-    const uint32_t s = smem_u32(src);
-    switch (P.tma_rank) {
-    case 1:
-        asm volatile("cp.async.bulk.tensor.1d.global.shared::cta.bulk_group [%0, {%1}], [%2];" ::"l"(map), "r"(c[0]), "r"(s)
-                     : "memory");
-        break;
-    case 2:
-        asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(map), "r"(c[0]),
-                     "r"(c[1]), "r"(s) : "memory");
-        break;
-    case 3:
-        asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(map),
-                     "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(s) : "memory");
-        break;
-    case 4:
-        asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.bulk_group [%0, {%1, %2, %3, %4}], [%5];" ::"l"(map),
-                     "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(s) : "memory");
-        break;
-    default:
-        asm volatile("cp.async.bulk.tensor.5d.global.shared::cta.bulk_group [%0, {%1, %2, %3, %4, %5}], [%6];" ::"l"(map),
-                     "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(c[4]), "r"(s) : "memory");
-        break;
-    }
-}
-
 template <typename V>
 __device__ __forceinline__ void issue_tile_load(const DenseLaunch& P, const V* s, V* buf, uint64_t* bar,
                                                 uint64_t item, int lane) {
@@ -189,9 +128,9 @@ __device__ __forceinline__ void issue_tile_load(const DenseLaunch& P, const V* s
     if (P.tma_rank) {
         if (lane == 0) {
             int32_t c[kTmaMaxRank];
-            tma_coords(P, base, c);
+            tma_box_coords(P.tma_rank, P.tma_lo, P.tma_len, P.tma_tile, base, c);
             mbar_arrive_expect_tx(bar, (uint32_t)sizeof(V) << (P.cols_bits + P.m));
-            tma_load(P, buf, bar, c);
+            tma_box_load(&P.tmap, P.tma_rank, smem_u32(buf), smem_u32(bar), c);
         }
         return;
     }
@@ -208,8 +147,8 @@ __device__ __forceinline__ void issue_tile_store(const DenseLaunch& P, V* s, con
     if (P.tma_rank) {
         if (lane == 0) {
             int32_t c[kTmaMaxRank];
-            tma_coords(P, base, c);
-            tma_store(P, buf, c);
+            tma_box_coords(P.tma_rank, P.tma_lo, P.tma_len, P.tma_tile, base, c);
+            tma_box_store(&P.tmap, P.tma_rank, smem_u32(buf), c);
             bulk_commit();
         }
         return;
@@ -449,6 +388,53 @@ bool dense_tma_enabled() {
     return on;
 }
 
+bool tile_map_dims(uint32_t tile_mask, int qubits, int32_t* lo, int32_t* len, int32_t* tile, int32_t* rank) {
+    // runs of tile / outer bits from bit 0 up; a tile run is split into boxes of at most 2^7
+    // elements for the innermost dimension (256 scalars) and 2^8 otherwise
+    int r = 0, b = 0;
+    while (b < qubits) {
+        const bool in = (tile_mask >> b) & 1u;
+        int n = 0;
+        while (b + n < qubits && (((tile_mask >> (b + n)) & 1u) != 0) == in) ++n;
+        int at = b;
+        while (n > 0) {
+            const int cap = in ? (r == 0 ? 7 : 8) : 32;
+            const int l = std::min(n, cap);
+            if (r == kDenseTmaMaxRank) return false;
+            lo[r] = at;
+            len[r] = l;
+            tile[r] = in ? 1 : 0;
+            ++r;
+            at += l;
+            n -= l;
+        }
+        b = at;
+    }
+    *rank = r;
+    return r > 0 && tile[0] == 1;
+}
+
+bool encode_tile_map(CUtensorMap* map, void* amps, int precision, int rank, const int32_t* lo, const int32_t* len,
+                     const int32_t* tile) {
+    auto encode = tensor_map_encoder();
+    if (!encode || rank < 1 || rank > kDenseTmaMaxRank) return false;
+    cuuint64_t dims[kDenseTmaMaxRank], strides[kDenseTmaMaxRank];
+    cuuint32_t box[kDenseTmaMaxRank], estr[kDenseTmaMaxRank];
+    const int elem = precision == QM_FP32 ? 8 : 16;
+    for (int d = 0; d < rank; ++d) {
+        dims[d] = (cuuint64_t)1 << len[d];
+        box[d] = tile[d] ? (cuuint32_t)1 << len[d] : 1u;
+        estr[d] = 1;
+        if (d > 0) strides[d - 1] = (cuuint64_t)elem << lo[d];
+    }
+    dims[0] *= 2;  // the innermost dimension counts scalars: (re, im) pairs
+    box[0] *= 2;
+    return encode(map, precision == QM_FP32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
+                  (cuuint32_t)rank, amps, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 bool dense_geometry(int qubits, int precision, const DenseOp& op, DenseGeometry& g) {
     const int m = op.m;
     if (m < 1 || m > kDenseMaxQubits || qubits < 9) return false;
@@ -480,35 +466,17 @@ bool dense_geometry(int qubits, int precision, const DenseOp& op, DenseGeometry&
     g.copy_mask = (qmask | lmask) & ~((1u << r) - 1u);
     g.copies = 1 << (tb - r);
     const int run_bytes = elem << r;
-    // tensor-map dimensions: runs of tile / outer bits from bit 0 up; a tile run is split into
-    // boxes of at most 2^7 elements for the innermost dimension (256 scalars) and 2^8 otherwise
+    // A tensor-map box is the unpadded natural order, whose column accesses are free of bank
+    // conflicts when the lowest index bits (a wavefront's worth: 8 complex128, 16 complex64) are
+    // column bits; otherwise only 1- and 2-qubit gates (too little arithmetic to mind) take it.
     g.tma_rank = 0;
     {
-        const uint32_t tile = qmask | lmask;
-        int rank = 0, b = 0;
-        bool ok = true;
-        while (b < qubits && ok) {
-            const bool in = (tile >> b) & 1u;
-            int len = 0;
-            while (b + len < qubits && (((tile >> (b + len)) & 1u) != 0) == in) ++len;
-            int lo = b;
-            while (len > 0) {
-                const int cap = in ? (rank == 0 ? 7 : 8) : 32;
-                const int l = std::min(len, cap);
-                if (rank == kDenseTmaMaxRank) {
-                    ok = false;
-                    break;
-                }
-                g.tma_lo[rank] = lo;
-                g.tma_len[rank] = l;
-                g.tma_tile[rank] = in ? 1 : 0;
-                ++rank;
-                lo += l;
-                len -= l;
-            }
-            b = lo;
-        }
-        if (ok && dense_tma_enabled()) g.tma_rank = rank;
+        const int low = precision == QM_FP32 ? 4 : 3;
+        const bool contiguous_columns = (lmask & ((1u << low) - 1u)) == ((1u << low) - 1u);
+        int32_t rank = 0;
+        if (dense_tma_enabled() && (contiguous_columns || m <= 2) &&
+            tile_map_dims(qmask | lmask, qubits, g.tma_lo, g.tma_len, g.tma_tile, &rank))
+            g.tma_rank = rank;
     }
     // padding keeps column accesses free of bank conflicts, but a tensor-map box is unpadded
     const int pad = (run_bytes >= 128 && g.tma_rank == 0) ? 16 / elem : 0;
@@ -566,27 +534,13 @@ cudaError_t launch_dense(void* amps, int qubits, int precision, const DenseOp& o
     P.m = op.m;
     P.tma_rank = 0;
     if (g.tma_rank) {
-        auto encode = tensor_map_encoder();
-        if (encode) {
-            cuuint64_t dims[kTmaMaxRank], strides[kTmaMaxRank];
-            cuuint32_t box[kTmaMaxRank], estr[kTmaMaxRank];
-            const int elem = precision == QM_FP32 ? 8 : 16;
+        if (encode_tile_map(&P.tmap, amps, precision, g.tma_rank, g.tma_lo, g.tma_len, g.tma_tile)) {
+            P.tma_rank = g.tma_rank;
             for (int d = 0; d < g.tma_rank; ++d) {
-                dims[d] = (cuuint64_t)1 << g.tma_len[d];
-                box[d] = g.tma_tile[d] ? (cuuint32_t)1 << g.tma_len[d] : 1u;
-                estr[d] = 1;
-                if (d > 0) strides[d - 1] = (cuuint64_t)elem << g.tma_lo[d];
                 P.tma_lo[d] = g.tma_lo[d];
                 P.tma_len[d] = g.tma_len[d];
                 P.tma_tile[d] = g.tma_tile[d];
             }
-            dims[0] *= 2;  // the innermost dimension counts scalars: (re, im) pairs
-            box[0] *= 2;
-            const CUresult cr =
-                encode(&P.tmap, precision == QM_FP32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64,
-                       (cuuint32_t)g.tma_rank, amps, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                       CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-            if (cr == CUDA_SUCCESS) P.tma_rank = g.tma_rank;
         }
         if (!P.tma_rank) {
             // no encoder: the unpadded layout's natural runs through bulk copies

@@ -14,8 +14,9 @@
 // three products hi*hi + hi*lo + lo*hi (the 3xTF32 scheme).  A's split is done once on the host.
 //
 // Per CTA (one per SM), for a ring of tiles of 64 rows x 32 columns (2048 amplitudes, 16 KiB):
-//   - bulk copies (cp.async.bulk, mbarrier completion) stage each tile into one of four buffers,
-//     three tiles ahead of the one being converted;
+//   - one tensor-map box (cp.async.bulk.tensor, natural index order) or bulk copies of runs
+//     (cp.async.bulk) stage each tile into one of four buffers, three tiles ahead of the one being
+//     converted, with mbarrier completion;
 //   - all 256 threads split the tile into B_hi / B_lo in the canonical K-major layout of the
 //     MMA (two B buffers, so tile i converts while tile i-1's MMAs run);
 //   - one thread issues the 24 MMAs of the tile (8 K-steps x 3 products, M = 128, N = 64, K = 8)
@@ -39,35 +40,37 @@ namespace qm {
 
 namespace {
 
-constexpr int kTcThreads = 256;
+constexpr int kTcThreads = 512;
 constexpr int kTcTileBits = 11;      // 64 rows x 32 columns
 constexpr int kTcCols = 32;          // complex columns per tile
 constexpr int kTcN = 2 * kTcCols;    // real columns of B and D
-constexpr int kTcStages = 4;         // staging buffers
+constexpr int kTcMaxStages = 5;      // staging buffers (4 where five do not fit)
 constexpr int kTmemCols = 2 * kTcN;  // two accumulators
 constexpr long long kTcWaitCycles = 2000000000ll;
-constexpr size_t kTcSmemMax = 220 * 1024;
+constexpr size_t kTcSmemMax = 226 * 1024;
 
 // shared-memory layout (bytes)
 constexpr int kAHalf = 128 * 64 * 4;           // one 128 x 64 TF32 operand image: 32 KiB
 // B, K-major without swizzle: core matrices of 8 real columns (n) x 4 rows (k, 16 bytes); the 16
 // k-groups of a column group 144 bytes apart (16 more than dense, so the conversion's stores of
-// k and k + 4 land in different banks), column groups 2304 bytes apart
+// k and k + 4 land in different banks), column groups 2320 bytes apart
 constexpr int kBLbo = 144;
-constexpr int kBSbo = 16 * kBLbo;              // 2304
-constexpr int kBHalf = (kTcN / 8) * kBSbo;     // one 64 x 64 B image: 18432 B
+constexpr int kBSbo = 16 * kBLbo + 16;         // 2320: column groups skewed by 16 bytes as well
+constexpr int kBHalf = (kTcN / 8) * kBSbo;     // one 64 x 64 B image: 18560 B
 constexpr int kOffA = 0;                       // A_hi, A_lo
 constexpr int kOffB = 2 * kAHalf;              // [2 buffers][hi, lo]
 constexpr int kOffStage = kOffB + 4 * kBHalf;  // staging ring, stage_bytes each
 
 struct TcLaunch {
+    CUtensorMap tmap;        // the tile as one box (tma_rank > 0), else bulk copies of runs
+    int32_t tma_rank, tma_lo[5], tma_len[5], tma_tile[5];
     const float* a_image;    // A_hi then A_lo, already in the MMA's K-major layout (64 KiB)
     int32_t* status;
     uint64_t items;
     uint32_t outer_mask, copy_mask;
     int32_t q_bits[6];
     int32_t l_bits[kTcTileBits];
-    int32_t cols_bits, run_bits, copies, stride, stage_elems, pad;
+    int32_t cols_bits, run_bits, copies, stride, stage_elems, stages;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -108,7 +111,8 @@ __device__ __forceinline__ void bulk_store(void* dst, const void* src, uint32_t 
                  : "memory");
 }
 __device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void bulk_wait_read() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// all bulk groups but the newest have finished reading their shared-memory sources
+__device__ __forceinline__ void bulk_wait_read_older() { asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory"); }
 __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
@@ -144,29 +148,55 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
                  : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
-    uint32_t r[32];
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
         : "r"(taddr));
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
 __device__ __forceinline__ int tile_weight(const TcLaunch& P, int g) {
     if (g < P.run_bits) return 1 << g;
     return P.stride << __popc(P.copy_mask & ((1u << g) - 1u));
 }
+// staged-tile offsets (amplitudes) of row b (fused-qubit index) and column j
+__device__ __forceinline__ int row_offset(const TcLaunch& P, int b) {
+    int w = 0;
+    for (int i = 0; i < 6; ++i)
+        if ((b >> i) & 1) w += tile_weight(P, P.q_bits[i]);
+    return w;
+}
+__device__ __forceinline__ int col_offset(const TcLaunch& P, int j) {
+    int w = 0;
+    for (int k = 0; k < P.cols_bits; ++k)
+        if ((j >> k) & 1) w += tile_weight(P, P.l_bits[k]);
+    return w;
+}
+// byte offset of (row b, complex column j) in a B image: real part in column n = 2j, imaginary
+// part 16 bytes on (column n + 1 of the same core matrix)
+__device__ __forceinline__ int b_image_offset(int b, int j) {
+    const int n = 2 * j;
+    return (n & 7) * 16 + (n >> 3) * kBSbo + (b & 3) * 4 + (b >> 2) * kBLbo;
+}
 
 __device__ __forceinline__ void issue_load(const TcLaunch& P, const float2* s, float2* buf, uint64_t* bar,
                                            uint64_t item, int lane) {
     const uint32_t base = deposit((uint32_t)item, P.outer_mask);
+    if (P.tma_rank) {
+        if (lane == 0) {
+            int32_t c[5];
+            tma_box_coords(P.tma_rank, P.tma_lo, P.tma_len, P.tma_tile, base, c);
+            mbar_arrive_expect_tx(bar, 8u << kTcTileBits);
+            tma_box_load(&P.tmap, P.tma_rank, smem_u32(buf), smem_u32(bar), c);
+        }
+        return;
+    }
     const uint32_t run_bytes = 8u << P.run_bits;
     if (lane == 0) mbar_arrive_expect_tx(bar, run_bytes * (uint32_t)P.copies);
     __syncwarp();
@@ -176,6 +206,15 @@ __device__ __forceinline__ void issue_load(const TcLaunch& P, const float2* s, f
 
 __device__ __forceinline__ void issue_store(const TcLaunch& P, float2* s, const float2* buf, uint64_t item, int lane) {
     const uint32_t base = deposit((uint32_t)item, P.outer_mask);
+    if (P.tma_rank) {
+        if (lane == 0) {
+            int32_t c[5];
+            tma_box_coords(P.tma_rank, P.tma_lo, P.tma_len, P.tma_tile, base, c);
+            tma_box_store(&P.tmap, P.tma_rank, smem_u32(buf), c);
+            bulk_commit();
+        }
+        return;
+    }
     const uint32_t run_bytes = 8u << P.run_bits;
     for (int x = lane; x < P.copies; x += 32)
         bulk_store(s + (base | deposit((uint32_t)x, P.copy_mask)), buf + (size_t)x * P.stride, run_bytes);
@@ -184,43 +223,61 @@ __device__ __forceinline__ void issue_store(const TcLaunch& P, float2* s, const 
 
 __device__ __forceinline__ float tf32_head(float x) { return __uint_as_float(__float_as_uint(x) & 0xffffe000u); }
 
+// kConvJ: column bit 0 is index bit 0 (the staged tile is contiguous along columns), which picks
+// the conversion's lane mapping and rotates the epilogue's stores (see below).
+template <bool kConvJ>
 __global__ void __launch_bounds__(kTcThreads, 1) k_dense_tc(float2* __restrict__ s, const __grid_constant__ TcLaunch P) {
     extern __shared__ __align__(1024) unsigned char smem[];
-    __shared__ uint64_t bar_load[kTcStages];
+    __shared__ uint64_t bar_load[kTcMaxStages];
     __shared__ uint64_t bar_mma[2];
     __shared__ uint64_t bar_a;
     __shared__ uint32_t tmem_base;
-    __shared__ int wq[64];
     __shared__ int abort_flag;
 
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const uint32_t S = (uint32_t)P.stages;
     float* a_img = reinterpret_cast<float*>(smem + kOffA);
     unsigned char* b_img = smem + kOffB;
     float2* stage = reinterpret_cast<float2*>(smem + kOffStage);
 
-    for (int b = t; b < 64; b += kTcThreads) {
-        int w = 0;
-        for (int i = 0; i < 6; ++i)
-            if ((b >> i) & 1) w += tile_weight(P, P.q_bits[i]);
-        wq[b] = w;
-    }
-    // conversion: thread t takes elements e = t + 256 * k (k < 8): b % 8 = e & 7, j = (e >> 3) & 31,
-    // b / 8 = e >> 8
-    int wl_conv = 0;
+    // Conversion: 4 elements per thread, element k at row b, column j_k = j_0 + 8k.  kConvJ: a
+    // warp takes 8 consecutive columns of 4 consecutive rows (j_0 = lane % 8, b = lane / 8 + 4 warp),
+    // so that its B-image stores of one core-matrix row fill all 32 banks; otherwise 32 consecutive
+    // rows of one column (b = lane + 32 (warp % 2), j_0 = warp / 2).  In both the B-image offset of
+    // element k is that of element 0 plus k * 2 SBO.
+    const int cb = kConvJ ? (lane >> 3) + 4 * warp : lane + 32 * (warp & 1);
+    const int cj = kConvJ ? (lane & 7) : (warp >> 1);
+    int conv_src[4];
     {
-        const int j = (t >> 3) & 31;
-        for (int k = 0; k < P.cols_bits; ++k)
-            if ((j >> k) & 1) wl_conv += tile_weight(P, P.l_bits[k]);
+        const int rb = row_offset(P, cb);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) conv_src[k] = rb + col_offset(P, cj + 8 * k);
     }
+    const int conv_dst = b_image_offset(cb, cj);
+
+    // Epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (rows r = 2a + p) and real columns
+    // 16 (w / 4) .. + 15, i.e. complex columns j = 8 (w / 4) + jj, jj < 8; the row pair (2a, 2a + 1)
+    // sits in adjacent lanes, p = 0 finishes jj = 0..3 and p = 1 jj = 4..7.  Where rows are
+    // multiples of 32 amplitudes apart (kConvJ layouts), every row of a warp would store the same
+    // column at once, all in one bank: step s stores column (s + a) % 4 instead.
+    const int er = (warp & 3) * 32 + lane, ea = er >> 1, ep = er & 1;
+    const int ejc = 8 * (warp >> 2) + 4 * ep;
+    int out_off[4];
+    {
+        const int base = row_offset(P, ea) + col_offset(P, ejc);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) out_off[q] = base + col_offset(P, kConvJ ? ((q + ea) & 3) : q);
+    }
+
     if (t == 0) {
-        for (int i = 0; i < kTcStages; ++i) mbar_init(&bar_load[i], 1);
+        for (uint32_t k = 0; k < S; ++k) mbar_init(&bar_load[k], 1);
         mbar_init(&bar_mma[0], 1);
         mbar_init(&bar_mma[1], 1);
         mbar_init(&bar_a, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         abort_flag = 0;
     }
-    if (warp == 0) {
+    if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
                      "r"((uint32_t)kTmemCols)
                      : "memory");
@@ -232,62 +289,59 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_dense_tc(float2* __restrict__
     const uint32_t tmem = tmem_base;
 
     const uint64_t step = gridDim.x;
-    uint64_t tiles = 0;
-    if ((uint64_t)blockIdx.x < P.items) tiles = (P.items - 1 - blockIdx.x) / step + 1;
+    uint32_t tiles = 0;
+    if ((uint64_t)blockIdx.x < P.items) tiles = (uint32_t)((P.items - 1 - blockIdx.x) / step + 1);
 
+    // the ring: tile i in buffer i % S; loads run S - 2 tiles ahead, so the buffer refilled in
+    // iteration i is the one whose store was issued in iteration i - 1 and only the newest store
+    // may still be reading shared memory
     if (warp == 0) {
         if (lane == 0) {
             mbar_arrive_expect_tx(&bar_a, 2u * kAHalf);
             bulk_load(a_img, P.a_image, 2u * kAHalf, &bar_a);
         }
-        for (int k = 0; k < kTcStages - 1; ++k)
-            if ((uint64_t)k < tiles)
-                issue_load(P, s, stage + (size_t)k * P.stage_elems, &bar_load[k], blockIdx.x + k * step, lane);
+        for (uint32_t k = 0; k + 2 < S; ++k)
+            if (k < tiles) issue_load(P, s, stage + (size_t)k * P.stage_elems, &bar_load[k], blockIdx.x + k * step, lane);
     }
     if (!mbar_wait_bounded(&bar_a, 0)) abort_flag = 1;
 
     const uint32_t a_base = smem_u32(a_img);
     const uint32_t b_base = smem_u32(b_img);
-    uint64_t i = 0;
+    uint32_t i = 0, cur = 0, prev = S - 1, lap = 0;  // cur = i % S, prev = (i - 1) % S, lap = i / S
     for (; i <= tiles; ++i) {
-        const int cur = (int)(i % kTcStages);
         const int bb = (int)(i & 1);
         if (i < tiles) {
             // 1. the tile has landed; 2. the MMAs that read this B buffer two tiles ago are done
-            bool ok = mbar_wait_bounded(&bar_load[cur], (uint32_t)(i / kTcStages) & 1u);
-            if (ok && i >= 2) ok = mbar_wait_bounded(&bar_mma[bb], (uint32_t)((i - 2) >> 1) & 1u);
+            bool ok = mbar_wait_bounded(&bar_load[cur], lap & 1u);
+            if (ok && i >= 2) ok = mbar_wait_bounded(&bar_mma[bb], ((i - 2) >> 1) & 1u);
             if (!ok) abort_flag = 1;
         }
         __syncthreads();
         if (abort_flag) break;
         if (i < tiles) {
-            // 3. split into the MMA's B layout: (k = b, n = 2j + c) at (n%8)*16 + (n/8)*SBO + (b%4)*4 + (b/4)*LBO
+            // 3. split into B_hi / B_lo in the MMA's K-major layout
             const float2* tile = stage + (size_t)cur * P.stage_elems;
-            unsigned char* bhi = b_img + (size_t)bb * 2 * kBHalf;
+            unsigned char* bhi = b_img + (size_t)bb * 2 * kBHalf + conv_dst;
             unsigned char* blo = bhi + kBHalf;
-            const int j = (t >> 3) & 31;
 #pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const int b = (t & 7) | (k << 3);
-                const float2 x = tile[wq[b] + wl_conv];
+            for (int k = 0; k < 4; ++k) {
+                const float2 x = tile[conv_src[k]];
                 float2 hi, lo;
                 hi.x = tf32_head(x.x);
                 hi.y = tf32_head(x.y);
                 lo.x = x.x - hi.x;
                 lo.y = x.y - hi.y;
-                const int n = 2 * j;  // real part in column n, imaginary part in column n + 1 (16 bytes on)
-                const int off = (n & 7) * 16 + (n >> 3) * kBSbo + (b & 3) * 4 + (b >> 2) * kBLbo;
-                *reinterpret_cast<float*>(bhi + off) = hi.x;
-                *reinterpret_cast<float*>(bhi + off + 16) = hi.y;
-                *reinterpret_cast<float*>(blo + off) = lo.x;
-                *reinterpret_cast<float*>(blo + off + 16) = lo.y;
+                *reinterpret_cast<float*>(bhi + k * 2 * kBSbo) = hi.x;
+                *reinterpret_cast<float*>(bhi + k * 2 * kBSbo + 16) = hi.y;
+                *reinterpret_cast<float*>(blo + k * 2 * kBSbo) = lo.x;
+                *reinterpret_cast<float*>(blo + k * 2 * kBSbo + 16) = lo.y;
             }
             fence_proxy_async();
         }
         tc_fence_before();
         __syncthreads();
         tc_fence_after();
-        if (i < tiles && t == 0) {
+        if (i < tiles && t == 32) {
             // 4. the tile's 24 MMAs into accumulator bb
             const uint32_t d = tmem + (uint32_t)(bb * kTcN);
             const uint32_t bhi = b_base + (uint32_t)(bb * 2 * kBHalf), blo = bhi + kBHalf;
@@ -304,82 +358,93 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_dense_tc(float2* __restrict__
             mma_commit(&bar_mma[bb]);
         }
         if (i >= 1) {
-            // 5. epilogue of the previous tile
-            const uint64_t pi = i - 1;
+            // 5. epilogue of the previous tile, over its own staging buffer
+            const uint32_t pi = i - 1;
             const int pb = (int)(pi & 1);
-            const int pst = (int)(pi % kTcStages);
-            if (!mbar_wait_bounded(&bar_mma[pb], (uint32_t)(pi >> 1) & 1u)) abort_flag = 1;
+            if (!mbar_wait_bounded(&bar_mma[pb], (pi >> 1) & 1u)) abort_flag = 1;
             tc_fence_after();
             __syncwarp();
-            float v[32];
-            const uint32_t col = (uint32_t)(pb * kTcN + (warp >> 2) * 32);
-            tmem_ld32(tmem + ((uint32_t)((warp & 3) * 32) << 16) + col, v);
-            // row r = 2a + p; columns n = 2j + c for j in [jc, jc + 16)
-            const int r = (warp & 3) * 32 + lane, a = r >> 1, p = r & 1;
-            const int jc = (warp >> 2) * 16;
-            float2* out = stage + (size_t)pst * P.stage_elems;
-            // p = 0 finishes j = jc .. jc+7, p = 1 finishes j = jc+8 .. jc+15
-            float other_re[8], other_im[8];
+            float v[16];
+            tmem_ld16(tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(pb * kTcN + (warp >> 2) * 16), v);
+            // v[2 jj], v[2 jj + 1] = D(r, 2 j), D(r, 2 j + 1); the partner row's values for the
+            // columns this lane finishes come over a shuffle
+            float other_re[4], other_im[4];
 #pragma unroll
-            for (int jj = 0; jj < 8; ++jj) {
-                const float send_re = p ? v[2 * jj] : v[2 * (jj + 8)];
-                const float send_im = p ? v[2 * jj + 1] : v[2 * (jj + 8) + 1];
-                other_re[jj] = __shfl_xor_sync(0xffffffffu, send_re, 1);
-                other_im[jj] = __shfl_xor_sync(0xffffffffu, send_im, 1);
+            for (int q = 0; q < 4; ++q) {
+                const float send_re = ep ? v[2 * q] : v[2 * (q + 4)];
+                const float send_im = ep ? v[2 * q + 1] : v[2 * (q + 4) + 1];
+                other_re[q] = __shfl_xor_sync(0xffffffffu, send_re, 1);
+                other_im[q] = __shfl_xor_sync(0xffffffffu, send_im, 1);
             }
             tc_fence_before();
+            float2 o[4];
 #pragma unroll
-            for (int jj = 0; jj < 8; ++jj) {
-                const int jl = p ? jj + 8 : jj;  // local column within this warp's 16
-                // own row: D(2a+p, 2j), D(2a+p, 2j+1); partner row: other_*
-                const float mre = p ? v[2 * (jj + 8)] : v[2 * jj];
-                const float mim = p ? v[2 * (jj + 8) + 1] : v[2 * jj + 1];
-                float2 o;
-                if (p == 0) {  // own = Re U row: out = (mre - other_im) + i (mim + other_re)
-                    o.x = mre - other_im[jj];
-                    o.y = mim + other_re[jj];
-                } else {       // own = Im U row, other = Re U row
-                    o.x = other_re[jj] - mim;
-                    o.y = other_im[jj] + mre;
+            for (int q = 0; q < 4; ++q) {
+                const float mre = ep ? v[2 * (q + 4)] : v[2 * q];
+                const float mim = ep ? v[2 * (q + 4) + 1] : v[2 * q + 1];
+                if (ep == 0) {  // own = Re U row: out = (mre - other_im) + i (mim + other_re)
+                    o[q].x = mre - other_im[q];
+                    o[q].y = mim + other_re[q];
+                } else {        // own = Im U row, other = Re U row
+                    o[q].x = other_re[q] - mim;
+                    o[q].y = other_im[q] + mre;
                 }
-                const int jg = jc + jl;
-                int w = 0;
-                for (int k = 0; k < P.cols_bits; ++k)
-                    if ((jg >> k) & 1) w += tile_weight(P, P.l_bits[k]);
-                out[wq[a] + w] = o;
             }
+            if (kConvJ) {  // o[s] <- o[(s + a) % 4]
+                if (ea & 1) {
+                    const float2 x0 = o[0];
+                    o[0] = o[1];
+                    o[1] = o[2];
+                    o[2] = o[3];
+                    o[3] = x0;
+                }
+                if (ea & 2) {
+                    const float2 x0 = o[0], x1 = o[1];
+                    o[0] = o[2];
+                    o[1] = o[3];
+                    o[2] = x0;
+                    o[3] = x1;
+                }
+            }
+            float2* out = stage + (size_t)prev * P.stage_elems;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) out[out_off[q]] = o[q];
             fence_proxy_async();
         }
         __syncthreads();
         if (warp == 0) {
-            if (i >= 1) issue_store(P, s, stage + (size_t)((i - 1) % kTcStages) * P.stage_elems,
-                                    blockIdx.x + (i - 1) * step, lane);
-            // 6. refill: tile i + stages - 1 goes into the buffer just stored from
-            const uint64_t nxt = i + kTcStages - 1;
+            if (i >= 1) issue_store(P, s, stage + (size_t)prev * P.stage_elems, blockIdx.x + (uint64_t)(i - 1) * step, lane);
+            // 6. refill: tile i + S - 2 into the buffer of tile i - 2 (its store was issued last iteration)
+            const uint32_t nxt = i + S - 2;
             if (nxt < tiles) {
-                bulk_wait_read();
+                const uint32_t nb = cur >= 2 ? cur - 2 : cur + S - 2;
+                bulk_wait_read_older();
                 fence_proxy_async();
                 __syncwarp();
-                issue_load(P, s, stage + (size_t)(nxt % kTcStages) * P.stage_elems, &bar_load[nxt % kTcStages],
-                           blockIdx.x + nxt * step, lane);
+                issue_load(P, s, stage + (size_t)nb * P.stage_elems, &bar_load[nb], blockIdx.x + (uint64_t)nxt * step,
+                           lane);
             }
+        }
+        prev = cur;
+        if (++cur == S) {
+            cur = 0;
+            ++lap;
         }
     }
     if (abort_flag) {
         if (t == 0) {
             atomicExch(P.status, (int32_t)QM_E_TIMEOUT);
-            // MMAs and loads already issued
-            for (uint64_t k = (i >= 1 ? i - 1 : 0); k < i + 1 && k < tiles; ++k)
-                mbar_wait_bounded(&bar_mma[k & 1], (uint32_t)(k >> 1) & 1u);
-            for (uint64_t k = i + 1; k < i + kTcStages && k < tiles; ++k)
-                mbar_wait_bounded(&bar_load[k % kTcStages], (uint32_t)(k / kTcStages) & 1u);
+            // the MMAs of tile i - 1 (issued, not yet waited on) and the loads in flight
+            if (i >= 1 && i - 1 < tiles) mbar_wait_bounded(&bar_mma[(i - 1) & 1], ((i - 1) >> 1) & 1u);
+            for (uint32_t k = i; k + 2 < i + S && k < tiles; ++k)
+                mbar_wait_bounded(&bar_load[k % S], (k / S) & 1u);
         }
     }
     if (warp == 0) bulk_wait_all();
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    if (warp == 0)
+    if (warp == 1)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)kTmemCols)
                      : "memory");
 }
@@ -451,22 +516,40 @@ cudaError_t launch_dense_tc(void* amps, int qubits, const DenseOp& op, const flo
     }
     for (int i = 0; i < 6; ++i) P.q_bits[i] = op.q[i];
     P.cols_bits = c;
+    // one tensor-map box per tile where the tile's bit runs fit five dimensions: the staged tile
+    // is then in natural index order (unpadded), and so are its runs for bulk copies without an
+    // encoder; otherwise padded runs in which every column bit lies below every fused bit
+    int32_t rank = 0;
+    const bool natural = dense_tma_enabled() && (qmask | lmask) & 1u &&
+                         tile_map_dims(qmask | lmask, qubits, P.tma_lo, P.tma_len, P.tma_tile, &rank);
+    if (natural) {
+        r = 0;
+        while (r < qubits && ((qmask | lmask) >> r & 1u)) ++r;
+        if (encode_tile_map(&P.tmap, amps, QM_FP32, rank, P.tma_lo, P.tma_len, P.tma_tile)) P.tma_rank = rank;
+    }
     P.run_bits = r;
     P.copy_mask = (qmask | lmask) & ~((1u << r) - 1u);
     P.copies = 1 << (kTcTileBits - r);
     const int run_bytes = 8 << r;
-    P.stride = (1 << r) + (run_bytes >= 128 ? 2 : 0);
+    P.stride = (1 << r) + (run_bytes >= 128 && !natural ? 2 : 0);
     P.stage_elems = ((P.copies * P.stride * 8 + 127) / 128) * 16;
     P.outer_mask = ((1u << qubits) - 1u) & ~(qmask | lmask);
     P.items = uint64_t(1) << (qubits - kTcTileBits);
-    const size_t smem = (size_t)kOffStage + (size_t)kTcStages * P.stage_elems * 8;
+    const size_t stage_bytes = (size_t)P.stage_elems * 8;
+    P.stages = kOffStage + kTcMaxStages * stage_bytes <= kTcSmemMax ? kTcMaxStages : kTcMaxStages - 1;
+    const size_t smem = (size_t)kOffStage + (size_t)P.stages * stage_bytes;
     if (smem > kTcSmemMax) return cudaErrorInvalidValue;
     std::call_once(once, [] {
-        attr = cudaFuncSetAttribute(k_dense_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmemMax);
+        attr = cudaFuncSetAttribute(k_dense_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmemMax);
+        if (attr == cudaSuccess)
+            attr = cudaFuncSetAttribute(k_dense_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTcSmemMax);
     });
     if (attr != cudaSuccess) return attr;
     const int grid = (int)std::min<uint64_t>(P.items, (uint64_t)std::max(1, sm_count));
-    k_dense_tc<<<grid, kTcThreads, smem, st>>>(reinterpret_cast<float2*>(amps), P);
+    if (lmask & 1u)
+        k_dense_tc<true><<<grid, kTcThreads, smem, st>>>(reinterpret_cast<float2*>(amps), P);
+    else
+        k_dense_tc<false><<<grid, kTcThreads, smem, st>>>(reinterpret_cast<float2*>(amps), P);
     return cudaGetLastError();
 }
 

@@ -59,6 +59,70 @@ __device__ __forceinline__ uint32_t deposit(uint32_t value, uint32_t mask) {
     return out;
 }
 
+// One tensor-map box (cp.async.bulk.tensor) between global and shared memory: `map` is the address
+// of a __grid_constant__ CUtensorMap, `rank` its dimensions (1..5), c the box coordinates.  The load
+// completes on the mbarrier at shared address `bar`; the store joins the thread's bulk group.
+__device__ __forceinline__ void tma_box_load(const void* map, int rank, uint32_t dst, uint32_t bar, const int32_t* c) {
+    const uint64_t m = reinterpret_cast<uint64_t>(map);
+    switch (rank) {
+    case 1:
+        asm volatile("cp.async.bulk.tensor.1d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2}], [%3];"
+                     ::"r"(dst), "l"(m), "r"(c[0]), "r"(bar) : "memory");
+        break;
+    case 2:
+        asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+                     ::"r"(dst), "l"(m), "r"(c[0]), "r"(c[1]), "r"(bar) : "memory");
+        break;
+    case 3:
+        asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+                     ::"r"(dst), "l"(m), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(bar) : "memory");
+        break;
+    case 4:
+        asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
+                     ::"r"(dst), "l"(m), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(bar) : "memory");
+        break;
+    default:
+        asm volatile("cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], [%7];"
+                     ::"r"(dst), "l"(m), "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(c[4]), "r"(bar) : "memory");
+        break;
+    }
+}
+
+__device__ __forceinline__ void tma_box_store(const void* map, int rank, uint32_t src, const int32_t* c) {
+    const uint64_t m = reinterpret_cast<uint64_t>(map);
+    switch (rank) {
+    case 1:
+        asm volatile("cp.async.bulk.tensor.1d.global.shared::cta.bulk_group [%0, {%1}], [%2];" ::"l"(m), "r"(c[0]), "r"(src)
+                     : "memory");
+        break;
+    case 2:
+        asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(m), "r"(c[0]),
+                     "r"(c[1]), "r"(src) : "memory");
+        break;
+    case 3:
+        asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(m), "r"(c[0]),
+                     "r"(c[1]), "r"(c[2]), "r"(src) : "memory");
+        break;
+    case 4:
+        asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.bulk_group [%0, {%1, %2, %3, %4}], [%5];" ::"l"(m),
+                     "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(src) : "memory");
+        break;
+    default:
+        asm volatile("cp.async.bulk.tensor.5d.global.shared::cta.bulk_group [%0, {%1, %2, %3, %4, %5}], [%6];" ::"l"(m),
+                     "r"(c[0]), "r"(c[1]), "r"(c[2]), "r"(c[3]), "r"(c[4]), "r"(src) : "memory");
+        break;
+    }
+}
+
+// Box coordinates of a work item whose outer index bits are `base`: 0 on tile dimensions, the
+// item's bits on the others.
+__device__ __forceinline__ void tma_box_coords(int rank, const int32_t* lo, const int32_t* len, const int32_t* tile,
+                                               uint32_t base, int32_t* c) {
+#pragma unroll
+    for (int d = 0; d < 5; ++d)
+        c[d] = (d < rank && !tile[d]) ? (int32_t)((base >> lo[d]) & ((1u << len[d]) - 1u)) : 0;
+}
+
 // Compensated FP64 accumulation (Neumaier): sum + comp carries the exact running total
 // to within one rounding of the largest partial.
 struct KSum {

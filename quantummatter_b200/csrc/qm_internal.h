@@ -2,6 +2,7 @@
 // libqmb200.so.  Not part of the public ABI (that is include/qm_b200.h).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -190,6 +191,12 @@ bool dense_geometry(int qubits, int precision, const DenseOp& op, DenseGeometry&
 // form at most five dimensions; QM_DENSE_TMA=0 keeps them on plain bulk copies.
 constexpr int kDenseTmaMaxRank = 5;
 bool dense_tma_enabled();
+// Tensor-map dimensions of a tile (the runs of tile and outer index bits from bit 0 up); false when
+// they need more than five.  encode_tile_map builds the map over the state at `amps` (tile runs at
+// full extent in the box, outer runs at extent 1); false without the driver's encoder.
+bool tile_map_dims(uint32_t tile_mask, int qubits, int32_t* lo, int32_t* len, int32_t* tile, int32_t* rank);
+bool encode_tile_map(CUtensorMap* map, void* amps, int precision, int rank, const int32_t* lo, const int32_t* len,
+                     const int32_t* tile);
 // One dense fused gate on a state (qm_dense.cu); `matrix` is its transposed unitary in device memory.
 cudaError_t launch_dense(void* amps, int qubits, int precision, const DenseOp& op, const double2* matrix,
                          int32_t* status, int sm_count, cudaStream_t s);
