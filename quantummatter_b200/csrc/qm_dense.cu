@@ -124,16 +124,16 @@ __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.
 template <typename V>
 __device__ __forceinline__ void issue_tile_load(const DenseLaunch& P, const V* s, V* buf, uint64_t* bar,
                                                 uint64_t item, int lane) {
-    const uint32_t base = deposit((uint32_t)item, P.outer_mask);
     if (P.tma_rank) {
         if (lane == 0) {
             int32_t c[kTmaMaxRank];
-            tma_box_coords(P.tma_rank, P.tma_lo, P.tma_len, P.tma_tile, base, c);
+            tma_item_coords(P.tma_rank, P.tma_len, P.tma_tile, (uint32_t)item, c);
             mbar_arrive_expect_tx(bar, (uint32_t)sizeof(V) << (P.cols_bits + P.m));
             tma_box_load(&P.tmap, P.tma_rank, smem_u32(buf), smem_u32(bar), c);
         }
         return;
     }
+    const uint32_t base = deposit((uint32_t)item, P.outer_mask);
     const uint32_t run_bytes = (uint32_t)sizeof(V) << P.xfer_bits;
     if (lane == 0) mbar_arrive_expect_tx(bar, run_bytes * (uint32_t)P.xfers);
     __syncwarp();
@@ -143,16 +143,16 @@ __device__ __forceinline__ void issue_tile_load(const DenseLaunch& P, const V* s
 
 template <typename V>
 __device__ __forceinline__ void issue_tile_store(const DenseLaunch& P, V* s, const V* buf, uint64_t item, int lane) {
-    const uint32_t base = deposit((uint32_t)item, P.outer_mask);
     if (P.tma_rank) {
         if (lane == 0) {
             int32_t c[kTmaMaxRank];
-            tma_box_coords(P.tma_rank, P.tma_lo, P.tma_len, P.tma_tile, base, c);
+            tma_item_coords(P.tma_rank, P.tma_len, P.tma_tile, (uint32_t)item, c);
             tma_box_store(&P.tmap, P.tma_rank, smem_u32(buf), c);
             bulk_commit();
         }
         return;
     }
+    const uint32_t base = deposit((uint32_t)item, P.outer_mask);
     const uint32_t run_bytes = (uint32_t)sizeof(V) << P.xfer_bits;
     for (int x = lane; x < P.xfers; x += 32)
         bulk_store(s + (base | deposit((uint32_t)x, P.xfer_mask)), buf + (size_t)x * P.xfer_stride, run_bytes);
@@ -211,6 +211,7 @@ __global__ void __launch_bounds__(kDenseThreads, 1)
         wl[i] = w;
     }
     if (t == 0) {
+        if (P.tma_rank) tma_prefetch(&P.tmap);
         for (int b = 0; b < P.nbuf; ++b) mbar_init(&bar[b], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         abort_flag = 0;

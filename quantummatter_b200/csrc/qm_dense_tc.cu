@@ -40,12 +40,16 @@ namespace qm {
 
 namespace {
 
-constexpr int kTcThreads = 512;
+constexpr int kTcConsumers = 512;                 // 16 warps: conversion and epilogue
+constexpr int kTcProducerWarp = kTcConsumers / 32;  // tile loads and stores
+constexpr int kTcMmaWarp = kTcProducerWarp + 1;     // TMEM allocation, A into TMEM order, MMAs
+constexpr int kTcThreads = kTcConsumers + 64;
 constexpr int kTcTileBits = 11;      // 64 rows x 32 columns
 constexpr int kTcCols = 32;          // complex columns per tile
 constexpr int kTcN = 2 * kTcCols;    // real columns of B and D
 constexpr int kTcMaxStages = 5;      // staging buffers (4 where five do not fit)
-constexpr int kTmemCols = 2 * kTcN;  // two accumulators
+constexpr int kTmemCols = 4 * kTcN;  // two accumulators, then A_hi and A_lo (64 columns each)
+constexpr int kTmemA = 2 * kTcN;     // first column of A_hi
 constexpr long long kTcWaitCycles = 2000000000ll;
 constexpr size_t kTcSmemMax = 226 * 1024;
 
@@ -134,12 +138,24 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
 constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kTcN >> 3) << 17) |
                             ((uint32_t)(128 >> 4) << 24);
 
-__device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t accumulate) {
+// D (TMEM) += A (TMEM: row m in lane m, K along columns) * B (shared memory descriptor)
+__device__ __forceinline__ void mma_tf32_ts(uint32_t d_tmem, uint32_t a_tmem, uint64_t b, uint32_t accumulate) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.u32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
-        "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate)
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "r"(a_tmem), "l"(b), "r"(kIdesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const float (&v)[32]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};" ::"r"(taddr),
+        "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7]), "f"(v[8]), "f"(v[9]),
+        "f"(v[10]), "f"(v[11]), "f"(v[12]), "f"(v[13]), "f"(v[14]), "f"(v[15]), "f"(v[16]), "f"(v[17]), "f"(v[18]),
+        "f"(v[19]), "f"(v[20]), "f"(v[21]), "f"(v[22]), "f"(v[23]), "f"(v[24]), "f"(v[25]), "f"(v[26]), "f"(v[27]),
+        "f"(v[28]), "f"(v[29]), "f"(v[30]), "f"(v[31])
         : "memory");
 }
 
@@ -187,16 +203,16 @@ __device__ __forceinline__ int b_image_offset(int b, int j) {
 
 __device__ __forceinline__ void issue_load(const TcLaunch& P, const float2* s, float2* buf, uint64_t* bar,
                                            uint64_t item, int lane) {
-    const uint32_t base = deposit((uint32_t)item, P.outer_mask);
     if (P.tma_rank) {
         if (lane == 0) {
             int32_t c[5];
-            tma_box_coords(P.tma_rank, P.tma_lo, P.tma_len, P.tma_tile, base, c);
+            tma_item_coords(P.tma_rank, P.tma_len, P.tma_tile, (uint32_t)item, c);
             mbar_arrive_expect_tx(bar, 8u << kTcTileBits);
             tma_box_load(&P.tmap, P.tma_rank, smem_u32(buf), smem_u32(bar), c);
         }
         return;
     }
+    const uint32_t base = deposit((uint32_t)item, P.outer_mask);
     const uint32_t run_bytes = 8u << P.run_bits;
     if (lane == 0) mbar_arrive_expect_tx(bar, run_bytes * (uint32_t)P.copies);
     __syncwarp();
@@ -205,16 +221,16 @@ __device__ __forceinline__ void issue_load(const TcLaunch& P, const float2* s, f
 }
 
 __device__ __forceinline__ void issue_store(const TcLaunch& P, float2* s, const float2* buf, uint64_t item, int lane) {
-    const uint32_t base = deposit((uint32_t)item, P.outer_mask);
     if (P.tma_rank) {
         if (lane == 0) {
             int32_t c[5];
-            tma_box_coords(P.tma_rank, P.tma_lo, P.tma_len, P.tma_tile, base, c);
+            tma_item_coords(P.tma_rank, P.tma_len, P.tma_tile, (uint32_t)item, c);
             tma_box_store(&P.tmap, P.tma_rank, smem_u32(buf), c);
             bulk_commit();
         }
         return;
     }
+    const uint32_t base = deposit((uint32_t)item, P.outer_mask);
     const uint32_t run_bytes = 8u << P.run_bits;
     for (int x = lane; x < P.copies; x += 32)
         bulk_store(s + (base | deposit((uint32_t)x, P.copy_mask)), buf + (size_t)x * P.stride, run_bytes);
@@ -223,16 +239,28 @@ __device__ __forceinline__ void issue_store(const TcLaunch& P, float2* s, const 
 
 __device__ __forceinline__ float tf32_head(float x) { return __uint_as_float(__float_as_uint(x) & 0xffffe000u); }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 // kConvJ: column bit 0 is index bit 0 (the staged tile is contiguous along columns), which picks
 // the conversion's lane mapping and rotates the epilogue's stores (see below).
+//
+// Roles, synchronised by mbarriers only (no block-wide barrier inside the tile loop):
+//   producer warp: tile i into buffer i % S (full[b]), S - 1 tiles ahead; stores tile i once its
+//     epilogue is written (done[b]) and reloads the buffer stored before it;
+//   MMA warp: after conv[bb] (tile i in B buffer bb) and accf[bb] (the epilogue of tile i - 2 has
+//     read accumulator bb), the tile's 24 MMAs, committed to mma[bb];
+//   16 consumer warps: convert tile i into B buffer i % 2 once mma[bb] shows tile i - 2's MMAs
+//     done, then the epilogue of tile i - 1 over its own staging buffer.
 template <bool kConvJ>
 __global__ void __launch_bounds__(kTcThreads, 1) k_dense_tc(float2* __restrict__ s, const __grid_constant__ TcLaunch P) {
     extern __shared__ __align__(1024) unsigned char smem[];
-    __shared__ uint64_t bar_load[kTcMaxStages];
-    __shared__ uint64_t bar_mma[2];
+    __shared__ uint64_t full[kTcMaxStages], done[kTcMaxStages];
+    __shared__ uint64_t conv[2], accf[2], mma[2];
     __shared__ uint64_t bar_a;
     __shared__ uint32_t tmem_base;
-    __shared__ int abort_flag;
+    __shared__ volatile int abort_flag;
 
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const uint32_t S = (uint32_t)P.stages;
@@ -240,44 +268,22 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_dense_tc(float2* __restrict__
     unsigned char* b_img = smem + kOffB;
     float2* stage = reinterpret_cast<float2*>(smem + kOffStage);
 
-    // Conversion: 4 elements per thread, element k at row b, column j_k = j_0 + 8k.  kConvJ: a
-    // warp takes 8 consecutive columns of 4 consecutive rows (j_0 = lane % 8, b = lane / 8 + 4 warp),
-    // so that its B-image stores of one core-matrix row fill all 32 banks; otherwise 32 consecutive
-    // rows of one column (b = lane + 32 (warp % 2), j_0 = warp / 2).  In both the B-image offset of
-    // element k is that of element 0 plus k * 2 SBO.
-    const int cb = kConvJ ? (lane >> 3) + 4 * warp : lane + 32 * (warp & 1);
-    const int cj = kConvJ ? (lane & 7) : (warp >> 1);
-    int conv_src[4];
-    {
-        const int rb = row_offset(P, cb);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) conv_src[k] = rb + col_offset(P, cj + 8 * k);
-    }
-    const int conv_dst = b_image_offset(cb, cj);
-
-    // Epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (rows r = 2a + p) and real columns
-    // 16 (w / 4) .. + 15, i.e. complex columns j = 8 (w / 4) + jj, jj < 8; the row pair (2a, 2a + 1)
-    // sits in adjacent lanes, p = 0 finishes jj = 0..3 and p = 1 jj = 4..7.  Where rows are
-    // multiples of 32 amplitudes apart (kConvJ layouts), every row of a warp would store the same
-    // column at once, all in one bank: step s stores column (s + a) % 4 instead.
-    const int er = (warp & 3) * 32 + lane, ea = er >> 1, ep = er & 1;
-    const int ejc = 8 * (warp >> 2) + 4 * ep;
-    int out_off[4];
-    {
-        const int base = row_offset(P, ea) + col_offset(P, ejc);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) out_off[q] = base + col_offset(P, kConvJ ? ((q + ea) & 3) : q);
-    }
-
     if (t == 0) {
-        for (uint32_t k = 0; k < S; ++k) mbar_init(&bar_load[k], 1);
-        mbar_init(&bar_mma[0], 1);
-        mbar_init(&bar_mma[1], 1);
+        if (P.tma_rank) tma_prefetch(&P.tmap);
+        for (uint32_t k = 0; k < S; ++k) {
+            mbar_init(&full[k], 1);
+            mbar_init(&done[k], kTcConsumers);
+        }
+        for (int k = 0; k < 2; ++k) {
+            mbar_init(&conv[k], kTcConsumers);
+            mbar_init(&accf[k], kTcConsumers);
+            mbar_init(&mma[k], 1);
+        }
         mbar_init(&bar_a, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         abort_flag = 0;
     }
-    if (warp == 1) {
+    if (warp == kTcMmaWarp) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
                      "r"((uint32_t)kTmemCols)
                      : "memory");
@@ -292,159 +298,227 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_dense_tc(float2* __restrict__
     uint32_t tiles = 0;
     if ((uint64_t)blockIdx.x < P.items) tiles = (uint32_t)((P.items - 1 - blockIdx.x) / step + 1);
 
-    // the ring: tile i in buffer i % S; loads run S - 2 tiles ahead, so the buffer refilled in
-    // iteration i is the one whose store was issued in iteration i - 1 and only the newest store
-    // may still be reading shared memory
-    if (warp == 0) {
+    if (warp == kTcProducerWarp) {
         if (lane == 0) {
             mbar_arrive_expect_tx(&bar_a, 2u * kAHalf);
             bulk_load(a_img, P.a_image, 2u * kAHalf, &bar_a);
         }
-        for (uint32_t k = 0; k + 2 < S; ++k)
-            if (k < tiles) issue_load(P, s, stage + (size_t)k * P.stage_elems, &bar_load[k], blockIdx.x + k * step, lane);
-    }
-    if (!mbar_wait_bounded(&bar_a, 0)) abort_flag = 1;
-
-    const uint32_t a_base = smem_u32(a_img);
-    const uint32_t b_base = smem_u32(b_img);
-    uint32_t i = 0, cur = 0, prev = S - 1, lap = 0;  // cur = i % S, prev = (i - 1) % S, lap = i / S
-    for (; i <= tiles; ++i) {
-        const int bb = (int)(i & 1);
-        if (i < tiles) {
-            // 1. the tile has landed; 2. the MMAs that read this B buffer two tiles ago are done
-            bool ok = mbar_wait_bounded(&bar_load[cur], lap & 1u);
-            if (ok && i >= 2) ok = mbar_wait_bounded(&bar_mma[bb], ((i - 2) >> 1) & 1u);
-            if (!ok) abort_flag = 1;
-        }
-        __syncthreads();
-        if (abort_flag) break;
-        if (i < tiles) {
-            // 3. split into B_hi / B_lo in the MMA's K-major layout
-            const float2* tile = stage + (size_t)cur * P.stage_elems;
-            unsigned char* bhi = b_img + (size_t)bb * 2 * kBHalf + conv_dst;
-            unsigned char* blo = bhi + kBHalf;
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const float2 x = tile[conv_src[k]];
-                float2 hi, lo;
-                hi.x = tf32_head(x.x);
-                hi.y = tf32_head(x.y);
-                lo.x = x.x - hi.x;
-                lo.y = x.y - hi.y;
-                *reinterpret_cast<float*>(bhi + k * 2 * kBSbo) = hi.x;
-                *reinterpret_cast<float*>(bhi + k * 2 * kBSbo + 16) = hi.y;
-                *reinterpret_cast<float*>(blo + k * 2 * kBSbo) = lo.x;
-                *reinterpret_cast<float*>(blo + k * 2 * kBSbo + 16) = lo.y;
+        uint32_t issued = 0;
+        for (; issued + 1 < S && issued < tiles; ++issued)
+            issue_load(P, s, stage + (size_t)issued * P.stage_elems, &full[issued], blockIdx.x + issued * step, lane);
+        uint32_t b = 0, lap = 0;
+        for (uint32_t j = 0; j < tiles; ++j) {
+            // lane 0 waits and decides for the warp: 0 go on, 1 another role stopped, 2 timed out
+            int st = 0;
+            if (lane == 0) st = abort_flag ? 1 : (mbar_wait_bounded(&done[b], lap & 1u) ? 0 : 2);
+            st = __shfl_sync(0xffffffffu, st, 0);
+            if (st) {
+                if (st == 2 && lane == 0) abort_flag = 1;
+                break;
             }
-            fence_proxy_async();
-        }
-        tc_fence_before();
-        __syncthreads();
-        tc_fence_after();
-        if (i < tiles && t == 32) {
-            // 4. the tile's 24 MMAs into accumulator bb
-            const uint32_t d = tmem + (uint32_t)(bb * kTcN);
-            const uint32_t bhi = b_base + (uint32_t)(bb * 2 * kBHalf), blo = bhi + kBHalf;
-#pragma unroll
-            for (int ks = 0; ks < 8; ++ks) {
-                const uint64_t ahi_d = smem_desc(a_base + ks * 256, 128, 2048);
-                const uint64_t alo_d = smem_desc(a_base + kAHalf + ks * 256, 128, 2048);
-                const uint64_t bhi_d = smem_desc(bhi + ks * 2 * kBLbo, kBLbo, kBSbo);
-                const uint64_t blo_d = smem_desc(blo + ks * 2 * kBLbo, kBLbo, kBSbo);
-                mma_tf32(d, ahi_d, bhi_d, ks > 0 ? 1u : 0u);
-                mma_tf32(d, ahi_d, blo_d, 1u);
-                mma_tf32(d, alo_d, bhi_d, 1u);
-            }
-            mma_commit(&bar_mma[bb]);
-        }
-        if (i >= 1) {
-            // 5. epilogue of the previous tile, over its own staging buffer
-            const uint32_t pi = i - 1;
-            const int pb = (int)(pi & 1);
-            if (!mbar_wait_bounded(&bar_mma[pb], (pi >> 1) & 1u)) abort_flag = 1;
-            tc_fence_after();
-            __syncwarp();
-            float v[16];
-            tmem_ld16(tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(pb * kTcN + (warp >> 2) * 16), v);
-            // v[2 jj], v[2 jj + 1] = D(r, 2 j), D(r, 2 j + 1); the partner row's values for the
-            // columns this lane finishes come over a shuffle
-            float other_re[4], other_im[4];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const float send_re = ep ? v[2 * q] : v[2 * (q + 4)];
-                const float send_im = ep ? v[2 * q + 1] : v[2 * (q + 4) + 1];
-                other_re[q] = __shfl_xor_sync(0xffffffffu, send_re, 1);
-                other_im[q] = __shfl_xor_sync(0xffffffffu, send_im, 1);
-            }
-            tc_fence_before();
-            float2 o[4];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const float mre = ep ? v[2 * (q + 4)] : v[2 * q];
-                const float mim = ep ? v[2 * (q + 4) + 1] : v[2 * q + 1];
-                if (ep == 0) {  // own = Re U row: out = (mre - other_im) + i (mim + other_re)
-                    o[q].x = mre - other_im[q];
-                    o[q].y = mim + other_re[q];
-                } else {        // own = Im U row, other = Re U row
-                    o[q].x = other_re[q] - mim;
-                    o[q].y = other_im[q] + mre;
-                }
-            }
-            if (kConvJ) {  // o[s] <- o[(s + a) % 4]
-                if (ea & 1) {
-                    const float2 x0 = o[0];
-                    o[0] = o[1];
-                    o[1] = o[2];
-                    o[2] = o[3];
-                    o[3] = x0;
-                }
-                if (ea & 2) {
-                    const float2 x0 = o[0], x1 = o[1];
-                    o[0] = o[2];
-                    o[1] = o[3];
-                    o[2] = x0;
-                    o[3] = x1;
-                }
-            }
-            float2* out = stage + (size_t)prev * P.stage_elems;
-#pragma unroll
-            for (int q = 0; q < 4; ++q) out[out_off[q]] = o[q];
-            fence_proxy_async();
-        }
-        __syncthreads();
-        if (warp == 0) {
-            if (i >= 1) issue_store(P, s, stage + (size_t)prev * P.stage_elems, blockIdx.x + (uint64_t)(i - 1) * step, lane);
-            // 6. refill: tile i + S - 2 into the buffer of tile i - 2 (its store was issued last iteration)
-            const uint32_t nxt = i + S - 2;
-            if (nxt < tiles) {
-                const uint32_t nb = cur >= 2 ? cur - 2 : cur + S - 2;
+            issue_store(P, s, stage + (size_t)b * P.stage_elems, blockIdx.x + (uint64_t)j * step, lane);
+            const uint32_t n = j + S - 1;
+            if (n < tiles) {
+                // the buffer of tile j - 1: all stores but the newest have read their buffers
+                const uint32_t nb = b == 0 ? S - 1 : b - 1;
                 bulk_wait_read_older();
                 fence_proxy_async();
                 __syncwarp();
-                issue_load(P, s, stage + (size_t)nb * P.stage_elems, &bar_load[nb], blockIdx.x + (uint64_t)nxt * step,
-                           lane);
+                issue_load(P, s, stage + (size_t)nb * P.stage_elems, &full[nb], blockIdx.x + (uint64_t)n * step, lane);
+                ++issued;
+            }
+            if (++b == S) {
+                b = 0;
+                ++lap;
             }
         }
-        prev = cur;
-        if (++cur == S) {
-            cur = 0;
-            ++lap;
+        // no load may still be writing shared memory when the block exits
+        for (uint32_t k = issued > S ? issued - S : 0; k < issued; ++k)
+            mbar_wait_bounded(&full[k % S], (k / S) & 1u);
+        bulk_wait_all();
+    } else if (warp == kTcMmaWarp) {
+        if (lane == 0) {
+            uint32_t issued = 0;
+            for (uint32_t i = 0; i < tiles; ++i) {
+                const int bb = (int)(i & 1);
+                bool ok = !abort_flag && mbar_wait_bounded(&conv[bb], (i >> 1) & 1u);
+                if (ok && i >= 2) ok = mbar_wait_bounded(&accf[bb], ((i - 2) >> 1) & 1u);
+                if (!ok) {
+                    abort_flag = 1;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t d = tmem + (uint32_t)(bb * kTcN);
+                const uint32_t bhi = smem_u32(b_img) + (uint32_t)(bb * 2 * kBHalf), blo = bhi + kBHalf;
+#pragma unroll
+                for (int ks = 0; ks < 8; ++ks) {
+                    const uint32_t ahi = tmem + (uint32_t)(kTmemA + 8 * ks), alo = ahi + 64u;
+                    const uint64_t bhi_d = smem_desc(bhi + ks * 2 * kBLbo, kBLbo, kBSbo);
+                    const uint64_t blo_d = smem_desc(blo + ks * 2 * kBLbo, kBLbo, kBSbo);
+                    mma_tf32_ts(d, ahi, bhi_d, ks > 0 ? 1u : 0u);
+                    mma_tf32_ts(d, ahi, blo_d, 1u);
+                    mma_tf32_ts(d, alo, bhi_d, 1u);
+                }
+                mma_commit(&mma[bb]);
+                ++issued;
+            }
+            // the MMAs still running when the loop ended early
+            for (uint32_t k = issued > 2 ? issued - 2 : 0; k < issued; ++k)
+                mbar_wait_bounded(&mma[k & 1], (k >> 1) & 1u);
+        }
+        __syncwarp();
+    } else {
+        // Conversion: 4 elements per thread, element k at row b, column j_k = j_0 + 8k.  kConvJ: a
+        // warp takes 8 consecutive columns of 4 consecutive rows (j_0 = lane % 8, b = lane / 8 +
+        // 4 warp), so that its B-image stores of one core-matrix row fill all 32 banks; otherwise
+        // 32 consecutive rows of one column (b = lane + 32 (warp % 2), j_0 = warp / 2).  In both
+        // the B-image offset of element k is that of element 0 plus k * 2 SBO.
+        const int cb = kConvJ ? (lane >> 3) + 4 * warp : lane + 32 * (warp & 1);
+        const int cj = kConvJ ? (lane & 7) : (warp >> 1);
+        int conv_src[4];
+        {
+            const int rb = row_offset(P, cb);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) conv_src[k] = rb + col_offset(P, cj + 8 * k);
+        }
+        const int conv_dst = b_image_offset(cb, cj);
+
+        // Epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 31 (rows r = 2a + p) and real columns
+        // 16 (w / 4) .. + 15, i.e. complex columns j = 8 (w / 4) + jj, jj < 8; the row pair
+        // (2a, 2a + 1) sits in adjacent lanes, p = 0 finishes jj = 0..3 and p = 1 jj = 4..7.  Where
+        // rows are multiples of 32 amplitudes apart (kConvJ layouts), every row of a warp would
+        // store the same column at once, all in one bank: step s stores column (s + a) % 4 instead.
+        const int er = (warp & 3) * 32 + lane, ea = er >> 1, ep = er & 1;
+        int out_off[4];
+        {
+            const int base = row_offset(P, ea) + col_offset(P, 8 * (warp >> 2) + 4 * ep);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) out_off[q] = base + col_offset(P, kConvJ ? ((q + ea) & 3) : q);
+        }
+        const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;
+
+        // A (the unitary's TF32 head and tail) into TMEM order: warps 0..7, row m = 32 (w % 4) +
+        // lane, head (w < 4) or tail, 64 K columns from the K-major shared-memory image
+        if (warp < 8) {
+            if (!__all_sync(0xffffffffu, mbar_wait_bounded(&bar_a, 0))) abort_flag = 1;
+            const float* img = a_img + (warp >> 2) * (kAHalf / 4);
+            const int m = er;
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                float v[32];
+#pragma unroll
+                for (int kk = 0; kk < 32; ++kk) {
+                    const int k = 32 * c + kk;
+                    v[kk] = img[(m >> 3) * 512 + (k >> 2) * 32 + (m & 7) * 4 + (k & 3)];
+                }
+                tmem_st32(tmem + lane_base + (uint32_t)(kTmemA + 64 * (warp >> 2) + 32 * c), v);
+            }
+            asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+        }
+
+        uint32_t cur = 0, prev = S - 1, lap = 0;  // cur = i % S, prev = (i - 1) % S, lap = i / S
+        // every stop below is decided for the whole warp (the TMEM loads and shuffles need all lanes)
+        for (uint32_t i = 0; i <= tiles; ++i) {
+            if (__any_sync(0xffffffffu, abort_flag != 0)) break;
+            if (i < tiles) {
+                const int bb = (int)(i & 1);
+                // the tile has landed, and the MMAs that read B buffer bb (tile i - 2) are done
+                bool ok = mbar_wait_bounded(&full[cur], lap & 1u);
+                if (ok && i >= 2) ok = mbar_wait_bounded(&mma[bb], ((i - 2) >> 1) & 1u);
+                if (!__all_sync(0xffffffffu, ok)) {
+                    abort_flag = 1;
+                    break;
+                }
+                const float2* tile = stage + (size_t)cur * P.stage_elems;
+                unsigned char* bhi = b_img + (size_t)bb * 2 * kBHalf + conv_dst;
+                unsigned char* blo = bhi + kBHalf;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const float2 x = tile[conv_src[k]];
+                    float2 hi, lo;
+                    hi.x = tf32_head(x.x);
+                    hi.y = tf32_head(x.y);
+                    lo.x = x.x - hi.x;
+                    lo.y = x.y - hi.y;
+                    *reinterpret_cast<float*>(bhi + k * 2 * kBSbo) = hi.x;
+                    *reinterpret_cast<float*>(bhi + k * 2 * kBSbo + 16) = hi.y;
+                    *reinterpret_cast<float*>(blo + k * 2 * kBSbo) = lo.x;
+                    *reinterpret_cast<float*>(blo + k * 2 * kBSbo + 16) = lo.y;
+                }
+                fence_proxy_async();
+                tc_fence_before();
+                mbar_arrive(&conv[bb]);
+            }
+            if (i >= 1) {
+                const uint32_t pi = i - 1;
+                const int pb = (int)(pi & 1);
+                if (!__all_sync(0xffffffffu, mbar_wait_bounded(&mma[pb], (pi >> 1) & 1u))) {
+                    abort_flag = 1;
+                    break;
+                }
+                tc_fence_after();
+                __syncwarp();
+                float v[16];
+                tmem_ld16(tmem + lane_base + (uint32_t)(pb * kTcN + (warp >> 2) * 16), v);
+                tc_fence_before();
+                mbar_arrive(&accf[pb]);
+                // v[2 jj], v[2 jj + 1] = D(r, 2 j), D(r, 2 j + 1); the partner row's values for
+                // the columns this lane finishes come over a shuffle
+                float other_re[4], other_im[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const float send_re = ep ? v[2 * q] : v[2 * (q + 4)];
+                    const float send_im = ep ? v[2 * q + 1] : v[2 * (q + 4) + 1];
+                    other_re[q] = __shfl_xor_sync(0xffffffffu, send_re, 1);
+                    other_im[q] = __shfl_xor_sync(0xffffffffu, send_im, 1);
+                }
+                float2 o[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const float mre = ep ? v[2 * (q + 4)] : v[2 * q];
+                    const float mim = ep ? v[2 * (q + 4) + 1] : v[2 * q + 1];
+                    if (ep == 0) {  // own = Re U row: out = (mre - other_im) + i (mim + other_re)
+                        o[q].x = mre - other_im[q];
+                        o[q].y = mim + other_re[q];
+                    } else {        // own = Im U row, other = Re U row
+                        o[q].x = other_re[q] - mim;
+                        o[q].y = other_im[q] + mre;
+                    }
+                }
+                if (kConvJ) {  // o[s] <- o[(s + a) % 4]
+                    if (ea & 1) {
+                        const float2 x0 = o[0];
+                        o[0] = o[1];
+                        o[1] = o[2];
+                        o[2] = o[3];
+                        o[3] = x0;
+                    }
+                    if (ea & 2) {
+                        const float2 x0 = o[0], x1 = o[1];
+                        o[0] = o[2];
+                        o[1] = o[3];
+                        o[2] = x0;
+                        o[3] = x1;
+                    }
+                }
+                float2* out = stage + (size_t)prev * P.stage_elems;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) out[out_off[q]] = o[q];
+                fence_proxy_async();
+                mbar_arrive(&done[prev]);
+            }
+            prev = cur;
+            if (++cur == S) {
+                cur = 0;
+                ++lap;
+            }
         }
     }
-    if (abort_flag) {
-        if (t == 0) {
-            atomicExch(P.status, (int32_t)QM_E_TIMEOUT);
-            // the MMAs of tile i - 1 (issued, not yet waited on) and the loads in flight
-            if (i >= 1 && i - 1 < tiles) mbar_wait_bounded(&bar_mma[(i - 1) & 1], ((i - 1) >> 1) & 1u);
-            for (uint32_t k = i; k + 2 < i + S && k < tiles; ++k)
-                mbar_wait_bounded(&bar_load[k % S], (k / S) & 1u);
-        }
-    }
-    if (warp == 0) bulk_wait_all();
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    if (warp == 1)
+    if (abort_flag && t == 0) atomicExch(P.status, (int32_t)QM_E_TIMEOUT);
+    if (warp == kTcMmaWarp)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)kTmemCols)
                      : "memory");
 }

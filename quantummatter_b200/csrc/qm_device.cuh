@@ -116,11 +116,23 @@ __device__ __forceinline__ void tma_box_store(const void* map, int rank, uint32_
 
 // Box coordinates of a work item whose outer index bits are `base`: 0 on tile dimensions, the
 // item's bits on the others.
-__device__ __forceinline__ void tma_box_coords(int rank, const int32_t* lo, const int32_t* len, const int32_t* tile,
-                                               uint32_t base, int32_t* c) {
+// Box coordinates of tile `item`: the tile's outer index bits, in increasing order, are the
+// concatenated coordinates of the box-size-1 dimensions (tile dimensions start at 0).
+__device__ __forceinline__ void tma_item_coords(int rank, const int32_t* len, const int32_t* tile, uint32_t item,
+                                                int32_t* c) {
+    int shift = 0;
 #pragma unroll
-    for (int d = 0; d < 5; ++d)
-        c[d] = (d < rank && !tile[d]) ? (int32_t)((base >> lo[d]) & ((1u << len[d]) - 1u)) : 0;
+    for (int d = 0; d < 5; ++d) {
+        const bool outer = d < rank && !tile[d];
+        const uint32_t mask = len[d] >= 32 ? 0xffffffffu : (1u << len[d]) - 1u;
+        c[d] = (outer && shift < 32) ? (int32_t)((item >> shift) & mask) : 0;
+        if (outer) shift += len[d];
+    }
+}
+
+// Brings a __grid_constant__ tensor map into the descriptor cache ahead of its first use.
+__device__ __forceinline__ void tma_prefetch(const void* map) {
+    asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
 }
 
 // Compensated FP64 accumulation (Neumaier): sum + comp carries the exact running total
