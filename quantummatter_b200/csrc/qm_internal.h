@@ -150,6 +150,7 @@ struct Plan {
     std::vector<const void*> jit;   // per pass: compiled kernel (cudaKernel_t) or null
     std::vector<std::vector<unsigned char>> jit_aux;  // per pass: the compiled kernel's constants
     std::vector<int> jit_tiles;     // per pass: shared-memory tiles of the compiled kernel (2: pipelined)
+    std::vector<int> jit_teams;     // per pass: teams of threads per block of the compiled kernel
     std::vector<int> jit_hist_bins; // per pass: bins of the compiled kernel's joint-mass epilogue (0: none)
     // Joint masses over these qubits (at most 8) are wanted after the plan (a damping group of the
     // trajectory runner): the last pass computes them in its epilogue when it compiles

@@ -231,6 +231,21 @@ struct Carry {
 constexpr int kMaxVariantBits = 5;      // pending sets one rotation may depend on at run time
 constexpr size_t kMaxAuxValues = 3000;  // constants per pass (kernel parameter space)
 
+// States of at least this many qubits copy the next work item's tile during the current one
+// (QM_PIPE_QUBITS overrides the 26; the CPU emulator of the generated kernels uses it to run the
+// pipelined forms on small states).
+int pipe_min_qubits() {
+    const char* e = std::getenv("QM_PIPE_QUBITS");
+    const int v = e ? std::atoi(e) : 0;
+    return v > 0 ? v : 26;
+}
+
+// Complex128 pipelined passes run as two teams per block (QM_TEAMS=0: one team, two blocks per SM).
+bool teams_enabled() {
+    const char* e = std::getenv("QM_TEAMS");
+    return !(e && e[0] == '0');
+}
+
 const char* kPrelude = R"SRC(
 typedef unsigned int u32;
 typedef unsigned long long u64;
@@ -263,6 +278,19 @@ __device__ __forceinline__ u32 qm_deposit(u32 value, u32 mask) {
     }
     return out;
 }
+#ifndef QM_EMULATED
+// tile copies (cp.async, no registers) and the named barriers of two-team blocks
+__device__ __forceinline__ void qm_cp16(u32 dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" :: "r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void qm_cp8(u32 dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" :: "r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void qm_cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void qm_cp_wait() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void qm_bar(u32 id, u32 n) { asm volatile("bar.sync %0, %1;" :: "r"(id), "r"(n) : "memory"); }
+__device__ __forceinline__ void qm_arrive(u32 id, u32 n) { asm volatile("bar.arrive %0, %1;" :: "r"(id), "r"(n) : "memory"); }
+#endif
 )SRC";
 
 struct Gen {
@@ -278,6 +306,8 @@ struct Gen {
     cplx G{1.0, 0.0};
     int uid = 0;
     uint32_t lanes = 0;  // lane order of the current layout (OP_STAGE `reserved`; 0: ascending)
+    // the block barrier of the exchanges (a team's named barrier in two-team blocks)
+    std::string bar = "__syncthreads();\n";
 
     std::string X(int i) const { return "x" + std::to_string(phys[i]); }
     std::string Y(int i) const { return "y" + std::to_string(phys[i]); }
@@ -387,7 +417,7 @@ struct Gen {
     }
 
     void stage(const int8_t* pos, uint32_t lane_code) {
-        os << "{ const u32 sb = qm_swz(base);\n__syncthreads();\n";
+        os << "{ const u32 sb = qm_swz(base);\n" << bar;
         for (int i = 0; i < NR; ++i) {
             os << "{ V v; v.x = " << X(i) << "; v.y = " << Y(i) << "; tile[sb ^ " << hexu(const_slot(i)) << "] = v; }\n";
         }
@@ -395,7 +425,7 @@ struct Gen {
         lanes = lane_code;
         for (int i = 0; i < NR; ++i) phys[i] = i;
         os << "base = " << base_expr() << ";\n";
-        os << "const u32 sn = qm_swz(base);\n__syncthreads();\n";
+        os << "const u32 sn = qm_swz(base);\n" << bar;
         for (int i = 0; i < NR; ++i)
             os << "{ const V v = tile[sn ^ " << hexu(const_slot(i)) << "]; x" << i << " = v.x; y" << i << " = v.y; }\n";
         os << "}\n";
@@ -875,7 +905,8 @@ struct Gen {
 struct Generated {
     std::string src;
     std::vector<unsigned char> aux;  // the parameter block: doubles (complex128) or floats
-    int tiles = 1;                   // tiles of shared memory (2: pipelined)
+    int tiles = 1;                   // tiles of shared memory (2: pipelined, or one per team)
+    int teams = 1;                   // teams of 2^(k - 4) threads per block
     int hist_bins = 0;               // joint-mass epilogue bins (0: none)
     bool zero_start = false;         // the pass writes |0...0> instead of loading the state
 };
@@ -939,34 +970,58 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int
     const int chunk = hist ? (qubits > 16 ? 1 << (16 - p.k) : 1 << (qubits - p.k)) : 1;
     const int warps = nt / 32;
     const size_t hist_bytes = hist ? sizeof(double) * (size_t)warps * hist_bins : 0;
-    const bool large = !tabled && !hist && !zero_start && qubits >= 26;
+    const bool large = !tabled && !hist && !zero_start && qubits >= pipe_min_qubits();
     const bool second = large && !fp64 && 2 * tile_bytes + prog_bytes <= (100u << 10);
     // Complex128: the exchange tile itself takes the next item's copy once the pass's last
     // exchange is done, so the copy overlaps the ops after it, the flush and the stores.
     const bool late = large && fp64;
     const bool piped = second || late;
-    int last_stage = -1;
+    int last_stage = -1, stages = 0;
     for (int o = 0; o < p.op_count; ++o)
-        if (plan_ops[(size_t)(p.op_begin + o)].code == OP_STAGE) last_stage = o;
-    const int tiles = second ? 2 : 1;
+        if (plan_ops[(size_t)(p.op_begin + o)].code == OP_STAGE) {
+            last_stage = o;
+            ++stages;
+        }
+    // Two teams per block (complex128 pipelined passes): the block is two teams of nt threads,
+    // each with its own tile and work items, synchronised by its own named barrier (1 + team).
+    // The teams take turns at the arithmetic: a team runs a compute segment (the ops between two
+    // exchanges) only while it holds the token, and hands it over before its next exchange, so
+    // one team's FP64 rotations overlap the other's shared-memory exchange and tile copy instead
+    // of both teams computing, then both exchanging.  The token is a pair of named barriers of
+    // both teams' threads: a team waits on its own (bar.sync) and signals the other's
+    // (bar.arrive).  Team 1 signals once up front, and team 0 takes one more token after its last
+    // item, so every barrier phase gets exactly its 2 nt arrivals; both teams run the same number
+    // of loop iterations and segments (a team without an item passes the token on unused).
+    const bool teams = late && teams_enabled() && 2 * nt <= 1024;
+    const int segs = stages + 1;
+    const std::string acquire = teams ? "qm_bar(tok_in, " + std::to_string(2 * nt) + "u);\n" : "";
+    const std::string release = teams ? "qm_arrive(tok_out, " + std::to_string(2 * nt) + "u);\n" : "";
+    if (teams) g.bar = "qm_bar(1u + team, " + std::to_string(nt) + "u);\n";
+    const int tiles = second || teams ? 2 : 1;
     // Blocks per SM: 128 registers per thread (512 threads per SM; fewer registers would spill
     // the 16 amplitudes) and the shared memory (a pipelined complex128 block of 12 qubits takes
     // an SM alone).
     const int minb =
-        std::max(1, std::min(512 / nt, (int)((220u << 10) / (tiles * tile_bytes + prog_bytes + 8192))));
+        teams ? 1 : std::max(1, std::min(512 / nt, (int)((220u << 10) / (tiles * tile_bytes + prog_bytes + 8192))));
     std::ostringstream& os = g.os;  // the kernel body
     os << "extern __shared__ __align__(16) unsigned char smem_raw[];\n";
-    os << "V* tile = reinterpret_cast<V*>(smem_raw);\n";
+    if (teams) {
+        os << "const u32 team = threadIdx.x >> " << p.k - R << ";\n";
+        os << "V* tile = reinterpret_cast<V*>(smem_raw + team * " << tile_bytes << "u);\n";
+    } else {
+        os << "V* tile = reinterpret_cast<V*>(smem_raw);\n";
+    }
     if (second) os << "V* ptile = reinterpret_cast<V*>(smem_raw + " << tile_bytes << ");\n";
     if (late) os << "V* ptile = tile;\n";
     if (hist) os << "double* hacc = reinterpret_cast<double*>(smem_raw + " << tiles * tile_bytes << ");\n";
     os << "FusedOp* prog = reinterpret_cast<FusedOp*>(smem_raw + " << tiles * tile_bytes + hist_bytes << ");\n";
     os << "double* table = reinterpret_cast<double*>(smem_raw + " << (tiles * tile_bytes + hist_bytes + prog_bytes)
        << ");\n";
-    os << "const u32 t = threadIdx.x;\n";
+    os << (teams ? "const u32 t = threadIdx.x & " + hexu((uint32_t)nt - 1u) + ";\n" : "const u32 t = threadIdx.x;\n");
     os << "{ const uint2* src = reinterpret_cast<const uint2*>(P.ops); uint2* dst = reinterpret_cast<uint2*>(prog);\n"
-       << "  for (int i = t; i < " << p.op_count * (int)(sizeof(FusedOp) / 8) << "; i += " << nt
+       << "  for (int i = threadIdx.x; i < " << p.op_count * (int)(sizeof(FusedOp) / 8) << "; i += " << nt * (teams ? 2 : 1)
        << ") dst[i] = __ldg(src + i); }\n";
+    if (teams) os << "__syncthreads();\n";  // both teams read the whole program
     os << "const long long total = (long long)P.states << P.cta_shift;\n";
     os << "const u32 cta_mask = (1u << P.cta_shift) - 1u;\n";
     // Tile pipeline: the next work item's tile is copied into `ptile` (cp.async, no registers)
@@ -987,24 +1042,31 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int
             for (int m = 0; m < R; ++m)
                 if ((r >> m) & 1) hi |= 1u << p.q[p.k - R + m];
             // slot of local index t + nt*r: the swizzle is linear, so qm_swz(t) ^ qm_swz(nt*r)
-            os << "asm volatile(\"cp.async." << (fp64 ? "cg" : "ca") << ".shared.global [%0], [%1], " << (fp64 ? 16 : 8)
-               << ";\" :: \"r\"(pf_b + ((pf_w ^ " << hexu(swz_host((uint32_t)(nt * r), fp64)) << ") << " << (fp64 ? 4 : 3)
-               << ")), \"l\"(src + " << hexu(hi) << ") : \"memory\");\n";
+            os << (fp64 ? "qm_cp16(" : "qm_cp8(") << "pf_b + ((pf_w ^ " << hexu(swz_host((uint32_t)(nt * r), fp64))
+               << ") << " << (fp64 ? 4 : 3) << "), src + " << hexu(hi) << ");\n";
         }
-        os << "}\nasm volatile(\"cp.async.commit_group;\" ::: \"memory\"); }\n";
+        os << "}\nqm_cp_commit(); }\n";
     };
-    prefetch("(long long)blockIdx.x");
+    // a team's work items: every other one of the block's (team 0 the even, team 1 the odd)
+    const char* next_item = teams ? "item + 2 * (long long)gridDim.x" : "item + gridDim.x";
+    prefetch(teams ? "(long long)blockIdx.x + (long long)team * gridDim.x" : "(long long)blockIdx.x");
     os << "int current = -1;\n";
     if (hist) {
         os << "for (long long u = blockIdx.x; u < total / " << chunk << "; u += gridDim.x) {\n";
         os << "for (int i = t; i < " << warps * hist_bins << "; i += " << nt << ") hacc[i] = 0.0;\n";
         os << "for (int cc = 0; cc < " << chunk << "; ++cc) {\nconst long long item = u * " << chunk << " + cc;\n";
+    } else if (teams) {
+        os << "const u32 tok_in = team ? 4u : 3u, tok_out = team ? 3u : 4u;\n";
+        os << "if (team == 1u) qm_arrive(3u, " << 2 * nt << "u);\n";
+        os << "for (long long k2 = 0; (long long)blockIdx.x + k2 * gridDim.x < total; k2 += 2) {\n";
+        os << "const long long item = (long long)blockIdx.x + (k2 + (long long)team) * gridDim.x;\n";
+        os << "if (item >= total) { for (int j = 0; j < " << segs << "; ++j) { " << acquire << release << "} continue; }\n";
     } else {
         os << "for (long long item = blockIdx.x; item < total; item += gridDim.x) {\n";
     }
     os << "const int b = (int)(item >> P.cta_shift);\nconst u32 cta = (u32)item & cta_mask;\n";
-    if (piped) os << "asm volatile(\"cp.async.wait_group 0;\" ::: \"memory\");\n";
-    os << "__syncthreads();\n";
+    if (piped) os << "qm_cp_wait();\n";
+    os << g.bar;
     if (tabled)
         os << "if (P.table_slots > 0 && b != current) { const double* row = P.table + (u64)b * P.table_stride;\n"
            << "  for (int i = t; i < 8 * P.table_slots; i += " << nt << ") table[i] = __ldg(row + i); __syncthreads(); }\n";
@@ -1022,9 +1084,10 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int
             os << "{ const V v = ptile[sn ^ " << hexu(g.const_slot(i)) << "]; x" << i << " = v.x; y" << i << " = v.y; }\n";
         os << "}\n";
         if (second || last_stage < 0) {
-            os << "__syncthreads();\n";
-            prefetch("item + gridDim.x");
+            os << g.bar;
+            prefetch(next_item);
         }
+        os << acquire;
     } else {
         os << "{ const u32 g0 = outer | " << deposit_expr("t", thread_in) << ";\n";
         for (int i = 0; i < NR; ++i) {
@@ -1043,11 +1106,13 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int
     for (int o = 0; o < p.op_count; ++o) {
         const FusedOp& op = plan_ops[(size_t)(p.op_begin + o)];
         if (op.code == OP_STAGE) {
+            os << release;
             g.stage(op.reg_pos, op.reserved);
             if (late && o == last_stage) {
-                os << "__syncthreads();\n";  // every thread has read the exchange tile
-                prefetch("item + gridDim.x");
+                os << g.bar;  // every thread has read the exchange tile
+                prefetch(next_item);
             }
+            os << acquire;
             continue;
         }
         if (op.code == OP_DIAG_GROUP) {
@@ -1126,6 +1191,7 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int
         }
         os << "}\n";
     }
+    os << release;
     os << "{ const u32 g1 = outer | " << permute_expr("t", p.out_bit, p.k - R) << ";\n";
     for (int i = 0; i < NR; ++i) {
         uint32_t gi = 0;
@@ -1134,6 +1200,7 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int
         os << "{ V v; v.x = " << g.X(i) << "; v.y = " << g.Y(i) << "; s[g1 | " << hexu(gi) << "] = v; }\n";
     }
     os << "}\n(void)base;\n}\n";
+    if (teams) os << "if (team == 0u) qm_bar(3u, " << 2 * nt << "u);\n";  // team 1's last hand-over
     if (hist) {
         os << "__syncthreads();\n";
         os << "for (int k = t; k < " << hist_bins << "; k += " << nt << ") { double sum = 0.0;\n"
@@ -1154,7 +1221,7 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int
               "& 15u); }\n";
     const size_t na = std::max<size_t>(1, g.aux.size());
     hd << "struct Aux { " << g.T << " v[" << na << "]; };\n";
-    hd << "extern \"C\" __global__ void __launch_bounds__(" << nt << ", " << minb
+    hd << "extern \"C\" __global__ void __launch_bounds__(" << nt * (teams ? 2 : 1) << ", " << minb
        << ") qm_pass(V* __restrict__ s0, const __grid_constant__ FusedLaunch P, const __grid_constant__ Aux A"
        << (hist ? ", double* __restrict__ hist" : "") << ") {\n";
     Generated out;
@@ -1162,6 +1229,7 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int
     if (g.aux.size() > kMaxAuxValues + 1000) return out;
     out.src = hd.str() + os.str();
     out.tiles = tiles;
+    out.teams = teams ? 2 : 1;
     out.hist_bins = hist_bins;
     out.zero_start = zero_start;
     if (fp64) {
@@ -1301,6 +1369,7 @@ void install(Plan& plan, std::vector<Generated>& gen, bool cached_only) {
         if (k) {
             plan.jit_aux[i] = std::move(gen[i].aux);
             plan.jit_tiles[i] = gen[i].tiles;
+            plan.jit_teams[i] = gen[i].teams;
             plan.jit_hist_bins[i] = gen[i].hist_bins;
         }
     }
@@ -1326,6 +1395,7 @@ void jit_prepare(Plan& plan) {
     plan.jit.assign(plan.passes.size(), nullptr);
     plan.jit_aux.assign(plan.passes.size(), {});
     plan.jit_tiles.assign(plan.passes.size(), 1);
+    plan.jit_teams.assign(plan.passes.size(), 1);
     plan.jit_hist_bins.assign(plan.passes.size(), 0);
     plan.hist_fused = false;
     plan.zero_fused = false;
@@ -1345,6 +1415,7 @@ void jit_lookup(Plan& plan) {
     plan.jit.assign(plan.passes.size(), nullptr);
     plan.jit_aux.assign(plan.passes.size(), {});
     plan.jit_tiles.assign(plan.passes.size(), 1);
+    plan.jit_teams.assign(plan.passes.size(), 1);
     plan.jit_hist_bins.assign(plan.passes.size(), 0);
     plan.hist_fused = false;
     plan.zero_fused = false;
@@ -1388,7 +1459,8 @@ cudaError_t launch_plan_pass(const Plan& plan, size_t pass, void* amps, const Fu
         return v;
     }();
     if (sms <= 0) return cudaErrorInvalidDevice;
-    const int threads = 1 << (p.k - R);
+    const int teams = pass < plan.jit_teams.size() ? plan.jit_teams[pass] : 1;
+    const int threads = teams << (p.k - R);
     int per_sm = 0;
     cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
     if (e != cudaSuccess) return e;

@@ -53,7 +53,8 @@ def _build(src: str) -> C.CDLL:
         tmp.replace(so)
     lib = C.CDLL(str(so))
     lib.emu_run.restype = C.c_int
-    lib.emu_run.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p, C.c_int]
+    lib.emu_run.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p, C.c_int,
+                            C.c_int, C.c_int]
     return lib
 
 
@@ -65,9 +66,9 @@ def _text(fn, *args) -> bytes:
     return buf.raw[:ln.value]
 
 
-def run_plan(circuit, precision: int, state: np.ndarray, width: int = 0) -> np.ndarray:
+def run_plan(circuit, precision: int, state: np.ndarray, width: int = 0, grid: int = 1) -> np.ndarray:
     """The plan's compiled passes (fusion width `width`, 0: the default) applied to a copy of
-    `state` on the CPU."""
+    `state` on the CPU, each launched as `grid` blocks."""
     n = circuit.QubitCount
     g, count = prepare(circuit)
     lib = load()
@@ -101,7 +102,9 @@ def run_plan(circuit, precision: int, state: np.ndarray, width: int = 0) -> np.n
         L.cta_shift = n - k
         L.states = 1
         auxbuf = C.create_string_buffer(aux, len(aux))
-        rc = _build(src).emu_run(s.ctypes.data, C.addressof(L), C.sizeof(L), auxbuf, len(aux), None, 1 << (k - R))
+        teams = 2 if "const u32 team = threadIdx.x >>" in src else 1
+        rc = _build(src).emu_run(s.ctypes.data, C.addressof(L), C.sizeof(L), auxbuf, len(aux), None,
+                                 teams << (k - R), teams, grid)
         if rc:
             raise RuntimeError(f"emulator rejected pass {i}: {rc}")
     return s

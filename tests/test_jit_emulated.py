@@ -94,3 +94,33 @@ def test_compiled_passes_on_the_cpu_match_the_oracle(name, make, precision, tol)
     got = je.run_plan(c, precision, psi)
     assert np.max(np.abs(got - want)) <= tol
     assert abs(np.linalg.norm(got) - math.sqrt(np.vdot(psi, psi).real)) <= 100 * tol
+
+
+PIPELINED = [
+    ("fp64_two_teams", FP64, "1", 1, 1e-12),
+    ("fp64_two_teams_idle_team", FP64, "1", 3, 1e-12),
+    ("fp64_one_team", FP64, "0", 2, 1e-12),
+    ("fp32_second_tile", FP32, "1", 3, 2e-5),
+]
+
+
+@pytest.mark.timeout(600)
+@pytest.mark.parametrize("name,precision,teams,grid,tol", PIPELINED, ids=[c[0] for c in PIPELINED])
+def test_pipelined_passes_on_the_cpu_match_the_oracle(monkeypatch, name, precision, teams, grid, tol):
+    """The forms of states of 26 qubits and more, generated here for 14 qubits (QM_PIPE_QUBITS):
+    the next tile copied during the current item, and for complex128 the block as two teams that
+    hand a compute token back and forth by named barriers.  With 3 blocks over 4 work items, two
+    blocks' team 1 has no item and must still pass the token on; a protocol whose arrivals do not
+    match hangs here (the timeout) rather than on a GPU."""
+    monkeypatch.setenv("QM_PIPE_QUBITS", "12")
+    monkeypatch.setenv("QM_TEAMS", teams)
+    c = brick_circuit(14, 12, seed=31)
+    from quantummatter_b200.circuit import prepare
+    g, n = prepare(c)
+    src = je._text(je.load().qm_jit_source, 14, precision, g, n, 0, 0).decode()
+    assert "qm_cp" in src
+    assert ("const u32 team = threadIdx.x >>" in src) == (precision == FP64 and teams == "1")
+    psi = random_state(14, 4)
+    want = orc.execute(c, psi)
+    got = je.run_plan(c, precision, psi, grid=grid)
+    assert np.max(np.abs(got - want)) <= tol
