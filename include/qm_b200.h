@@ -274,6 +274,10 @@ int32_t qm_plan_program(int32_t qubits, int32_t precision, const qm_gate* gates,
  * process-wide counts; qm_jit_source returns the generated source of one pass of the plan the
  * planner makes for `gates` (length receives the full size). */
 int32_t qm_jit_info(int32_t* available, int64_t* kernels, int64_t* failed, int64_t* launches);
+/* Dense fused gates (fusion widths 2..6): how many kernel launches the process has made, and how
+ * many of them ran on the tensor cores (complex64 gates of 5 and 6 qubits in states of 11 qubits or
+ * more; QM_DENSE_TC=0 in the environment at planning keeps them on the FP32 pipes).  Additive. */
+int32_t qm_dense_info(int64_t* launches, int64_t* tensor_core_launches);
 int32_t qm_jit_source(int32_t qubits, int32_t precision, const qm_gate* gates, int32_t count,
                       int32_t fusion_width, int32_t pass, char* buffer, size_t size, size_t* length);
 /* The constant parameter block that the same compiled pass is launched with (the rotation and

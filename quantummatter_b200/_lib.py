@@ -195,6 +195,7 @@ SIGNATURES = {
     "qm_marginal_probability": (I32, [P, I32P, I32, I32, DP]),
     "qm_measure": (I32, [P, I32P, I32, C.c_double, I32P, I32P]),
     "qm_jit_info": (I32, [I32P, I64P, I64P, I64P]),
+    "qm_dense_info": (I32, [I64P, I64P]),
     "qm_jit_source": (I32, [I32, I32, C.POINTER(Gate), I32, I32, I32, C.c_char_p, C.c_size_t,
                             C.POINTER(C.c_size_t)]),
     "qm_jit_constants": (I32, [I32, I32, C.POINTER(Gate), I32, I32, I32, C.c_void_p, C.c_size_t,

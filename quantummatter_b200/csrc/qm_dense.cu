@@ -23,6 +23,8 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include <algorithm>
 #include <cstdlib>
 #include <mutex>
@@ -503,11 +505,14 @@ bool dense_geometry(int qubits, int precision, const DenseOp& op, DenseGeometry&
     return true;
 }
 
+std::atomic<int64_t> g_dense_launches{0}, g_dense_tc_launches{0};
+
 cudaError_t launch_dense(void* amps, int qubits, int precision, const DenseOp& op, const double2* matrix,
                          int32_t* status, int sm_count, cudaStream_t st) {
     uint32_t qmask = 0;
     for (int i = 0; i < op.m; ++i) qmask |= 1u << op.q[i];
     if (qubits < 9) {
+        g_dense_launches.fetch_add(1, std::memory_order_relaxed);
         if (precision == QM_FP32)
             k_dense_small<float><<<1, 256, 0, st>>>(reinterpret_cast<float2*>(amps), matrix, qmask, op.m, qubits);
         else
@@ -561,6 +566,7 @@ cudaError_t launch_dense(void* amps, int qubits, int precision, const DenseOp& o
     P.buf_elems = g.buf_elems;
     P.buf_offset = g.buf_offset;
     const int grid = (int)std::min<uint64_t>(g.items, (uint64_t)std::max(1, sm_count));
+    g_dense_launches.fetch_add(1, std::memory_order_relaxed);
     // 16 outputs per thread: 256 threads for a 4096-amplitude tile, 32 for the 512 of a 9-qubit state
     const int threads = 1 << (g.cols_bits + op.m - 4);
     if (precision == QM_FP32) return launch_dense_t<float>(amps, op.m, P, grid, threads, g.smem, st);
@@ -568,3 +574,11 @@ cudaError_t launch_dense(void* amps, int qubits, int precision, const DenseOp& o
 }
 
 }  // namespace qm
+
+// Launch counts of the dense fused-gate kernels since the library was loaded: all of them, and
+// those that ran on the tensor cores.
+extern "C" int32_t qm_dense_info(int64_t* launches, int64_t* tensor_core_launches) {
+    if (launches) *launches = qm::g_dense_launches.load() + qm::g_dense_tc_launches.load();
+    if (tensor_core_launches) *tensor_core_launches = qm::g_dense_tc_launches.load();
+    return QM_OK;
+}

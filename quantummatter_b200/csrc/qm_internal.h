@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -204,6 +205,7 @@ cudaError_t launch_dense(void* amps, int qubits, int precision, const DenseOp& o
 // 6-qubit fused gates on complex64 states of at least 11 qubits run on the tensor cores
 // (qm_dense_tc.cu, 3xTF32) when QM_DENSE_TC=1; otherwise they stay on the FP32 pipes.
 bool dense_tc_enabled();
+extern std::atomic<int64_t> g_dense_launches, g_dense_tc_launches;  // launch counts (qm_dense_info)
 bool dense_tc_supported(int qubits, int precision, const DenseOp& op);
 void dense_tc_image(const double* transposed_unitary, std::vector<float>& image);
 cudaError_t launch_dense_tc(void* amps, int qubits, const DenseOp& op, const float* a_image, int32_t* status,

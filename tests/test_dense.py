@@ -121,3 +121,89 @@ def test_dense_fused_gates_on_every_qubit_placement(gpu_context):
                 st.Upload(psi)
                 st.Evolve(c, fusion_width=len(qubits))
                 assert np.max(np.abs(st.Download() - want)) <= tol, (qubits, precision)
+
+
+def dense_launches() -> tuple[int, int]:
+    """(dense fused-gate launches, of which on the tensor cores) since the library loaded."""
+    a, b = C.c_int64(), C.c_int64()
+    check(load().qm_dense_info(C.byref(a), C.byref(b)))
+    return a.value, b.value
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("width", [5, 6])
+@pytest.mark.parametrize("n", [11, 12, 14, 20])
+def test_tensor_core_dense_gates_match_the_oracle(gpu_context, monkeypatch, n, width):
+    """Complex64 fused gates of 5 and 6 qubits on the tensor cores (tcgen05, 3xTF32 split,
+    QM_DENSE_TC=1; 5-qubit gates widened by one qubit) against the oracle at the FP32 tolerance,
+    with the tensor-core kernel shown to have run.  11 qubits is a single tile."""
+    monkeypatch.setenv("QM_DENSE_TC", "1")
+    c = random_circuit(n, 160, seed=7000 + 100 * width + n)
+    psi = random_state(n, n + width + 50)
+    want = orc.execute(c, psi)
+    _, tc0 = dense_launches()
+    with DeviceState(gpu_context, n, FP32) as st:
+        st.Upload(psi)
+        st.Evolve(c, fusion_width=width)
+        got = st.Download()
+    _, tc1 = dense_launches()
+    assert tc1 > tc0
+    assert np.max(np.abs(got - want)) <= 2e-6
+
+
+@pytest.mark.gpu
+def test_tensor_core_dense_gates_on_every_qubit_placement(gpu_context, monkeypatch):
+    """Tensor-core fused gates whose qubits sit at the bottom (the tile contiguous along its
+    columns), the top and scattered, and the benchmark's brick through a persistent plan."""
+    monkeypatch.setenv("QM_DENSE_TC", "1")
+    n = 16
+    rng = np.random.default_rng(5)
+    for qubits in ([0, 1, 2, 3, 4, 5], [10, 11, 12, 13, 14, 15], [1, 3, 5, 7, 9, 11], [0, 5, 6, 12, 15, 2],
+                   [4, 5, 6, 7, 8]):
+        c = QuantumCircuit(n)
+        for _ in range(3):
+            for q in qubits:
+                c.Ry(q, float(rng.uniform(0, 6.28))).Rz(q, float(rng.uniform(0, 6.28)))
+            for a, b in zip(qubits, qubits[1:]):
+                c.CNot(a, b)
+        psi = random_state(n, len(qubits) + 90)
+        want = orc.execute(c, psi)
+        _, tc0 = dense_launches()
+        with DeviceState(gpu_context, n, FP32) as st:
+            st.Upload(psi)
+            st.Evolve(c, fusion_width=len(qubits))
+            got = st.Download()
+        assert dense_launches()[1] > tc0, qubits
+        assert np.max(np.abs(got - want)) <= 2e-6, qubits
+    n = 22
+    c = brick_circuit(n, 6, seed=11)
+    want = orc.execute_parallel(c)
+    _, tc0 = dense_launches()
+    plan = Plan(gpu_context, c, FP32, fusion_width=6)
+    try:
+        with DeviceState(gpu_context, n, FP32) as st:
+            plan.execute(st)
+            got = st.Download()
+    finally:
+        plan.Dispose()
+    assert dense_launches()[1] > tc0
+    assert np.max(np.abs(got - want)) <= 2e-6
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("width", [5, 6])
+@pytest.mark.parametrize("n", [12, 20])
+def test_fp32_pipe_dense_gates_match_the_oracle(gpu_context, monkeypatch, n, width):
+    """With QM_DENSE_TC=0 the complex64 gates of 5 and 6 qubits stay on the FP32 pipes (k_dense)."""
+    monkeypatch.setenv("QM_DENSE_TC", "0")
+    c = random_circuit(n, 160, seed=8000 + 100 * width + n)
+    psi = random_state(n, n + width + 70)
+    want = orc.execute(c, psi)
+    launches0, tc0 = dense_launches()
+    with DeviceState(gpu_context, n, FP32) as st:
+        st.Upload(psi)
+        st.Evolve(c, fusion_width=width)
+        got = st.Download()
+    launches1, tc1 = dense_launches()
+    assert tc1 == tc0 and launches1 > launches0
+    assert np.max(np.abs(got - want)) <= 2e-6
