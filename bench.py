@@ -222,7 +222,8 @@ def vqe_side_run(ctx, qubits: int = 22, vectors: int = 16) -> dict:
     """A bounded batched-variational run beside the headline: the hardware-efficient ansatz (4
     layers) on a `qubits`-site XXZ chain, `vectors` parameter vectors with full parameter-shift
     gradients, FP32 and FP64 batched, against the plain form (one FP64 circuit at a time on a
-    resident state); warm-up with the full batch so no compilation or graph capture is timed."""
+    resident state); warm-up with the full batch so no compilation or graph capture is timed, then
+    the faster of two timed calls."""
     import numpy as np
 
     from quantummatter_b200.backend import FP32, FP64, DeviceState
@@ -235,11 +236,14 @@ def vqe_side_run(ctx, qubits: int = 22, vectors: int = 16) -> dict:
     for name, prec in (("fp32", FP32), ("fp64", FP64)):
         ev = B200VariationalEnergyEvaluator(ctx, prec)
         ev.EvaluateBatch(c, h, params, withGradient=True)
-        t0 = time.perf_counter()
-        r = ev.EvaluateBatch(c, h, params, withGradient=True)
-        dt = time.perf_counter() - t0
+        best = None
+        for _ in range(2):  # one call is about a second of wall time: keep the faster of two
+            t0 = time.perf_counter()
+            r = ev.EvaluateBatch(c, h, params, withGradient=True)
+            dt = time.perf_counter() - t0
+            best = dt if best is None else min(best, dt)
         res[name] = r
-        out[f"batched_{name}_evals_per_s"] = r.Circuits / dt
+        out[f"batched_{name}_evals_per_s"] = r.Circuits / best
     bound = [c.Bind(list(params[0]))] + [c.BindWithRotationShift(list(params[0]), r, s)
                                          for r in range(8) for s in (np.pi / 2, -np.pi / 2)]
     with DeviceState(ctx, qubits, FP64) as st:

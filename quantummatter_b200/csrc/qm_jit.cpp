@@ -1002,7 +1002,8 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int
     // the 16 amplitudes) and the shared memory (a pipelined complex128 block of 12 qubits takes
     // an SM alone).
     const int minb =
-        teams ? 1 : std::max(1, std::min(512 / nt, (int)((220u << 10) / (tiles * tile_bytes + prog_bytes + 8192))));
+        teams ? std::max(1, 512 / (2 * nt))
+              : std::max(1, std::min(512 / nt, (int)((220u << 10) / (tiles * tile_bytes + prog_bytes + 8192))));
     std::ostringstream& os = g.os;  // the kernel body
     os << "extern __shared__ __align__(16) unsigned char smem_raw[];\n";
     if (teams) {
