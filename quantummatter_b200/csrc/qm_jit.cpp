@@ -582,8 +582,21 @@ struct Gen {
     struct PairPhase {
         int cls = 0;
         std::string re[NR], im[NR];
+        // shear form (rotations only): the pair's phase known at compile time as i^quad exp(i a),
+        // |a| <= pi/4, applied to y as three shears with tan(a / 2) and sin(a) (names in re / im)
+        bool shear[NR] = {};
+        int quad[NR] = {};
     };
-    PairPhase take_phase(int q, cplx extra) {
+    // One phase value as i^quad exp(i a), |a| <= pi/4: its shear constants tan(a / 2), sin(a).
+    void shear_constants(cplx v, int& quad, int& st, int& ss) {
+        double a = std::arg(v);
+        const double q = std::nearbyint(a / (M_PI / 2));
+        a -= q * (M_PI / 2);
+        quad = ((int)q % 4 + 4) % 4;
+        st = slot(std::tan(a / 2));
+        ss = slot(std::sin(a));
+    }
+    PairPhase take_phase(int q, cplx extra, bool shears = false) {
         PairPhase P;
         cplx ls = extra;
         std::vector<Pend> dep, keep;
@@ -614,10 +627,22 @@ struct Gen {
                 P.cls = 1;
                 return P;
             }
-            const int s = slot2(ls);
             const std::string n = "l" + std::to_string(uid++);
-            os << "const " << T << " " << n << "r = " << av(s) << ", " << n << "i = " << av(s + 1) << ";\n";
             P.cls = 2;
+            if (shears) {
+                int quad, st, ss;
+                shear_constants(ls, quad, st, ss);
+                os << "const " << T << " " << n << "a = " << av(st) << ", " << n << "b = " << av(ss) << ";\n";
+                for (int i = 0; i < NR; ++i) {
+                    P.re[i] = n + "a";
+                    P.im[i] = n + "b";
+                    P.shear[i] = true;
+                    P.quad[i] = quad;
+                }
+                return P;
+            }
+            const int s = slot2(ls);
+            os << "const " << T << " " << n << "r = " << av(s) << ", " << n << "i = " << av(s + 1) << ";\n";
             for (int i = 0; i < NR; ++i) {
                 P.re[i] = n + "r";
                 P.im[i] = n + "i";
@@ -625,21 +650,42 @@ struct Gen {
             return P;
         }
         const int J = (int)dep.size();
-        const int first = (int)aux.size();
-        for (int key = 0; key < (1 << J); ++key) {
+        auto variant = [&](int key) {
             cplx v = ls;
             for (int d = 0; d < J; ++d) v *= ((key >> d) & 1) ? std::conj(dep[d].v) : dep[d].v;
-            slot2(v);
-        }
+            return v;
+        };
         std::string kr;
         for (int d = 0; d < J; ++d) {
             const std::string e = sel_expr(dep[d].lmask, dep[d].omask);
             if (!e.empty()) kr += (kr.empty() ? "(" : " | (") + e + " << " + std::to_string(d) + ")";
         }
         const std::string id = std::to_string(uid++);
-        if (!kr.empty()) os << "const int k" << id << " = " << kr << ";\n";
         P.cls = 2;
         std::string declared[1 << kMaxVariantBits];
+        if (shears && kr.empty()) {  // every pair's variant is fixed by its register bits
+            int quads[1 << kMaxVariantBits];
+            for (int i = 0; i < NR; ++i) {
+                int rk = 0;
+                for (int d = 0; d < J; ++d)
+                    if (__builtin_popcount((uint32_t)i & reg_part(dep[d].lmask)) & 1) rk |= 1 << d;
+                if (declared[rk].empty()) {
+                    int st, ss;
+                    shear_constants(variant(rk), quads[rk], st, ss);
+                    const std::string n = "l" + id + "_" + std::to_string(rk);
+                    os << "const " << T << " " << n << "a = " << av(st) << ", " << n << "b = " << av(ss) << ";\n";
+                    declared[rk] = n;
+                }
+                P.re[i] = declared[rk] + "a";
+                P.im[i] = declared[rk] + "b";
+                P.shear[i] = true;
+                P.quad[i] = quads[rk];
+            }
+            return P;
+        }
+        const int first = (int)aux.size();
+        for (int key = 0; key < (1 << J); ++key) slot2(variant(key));
+        if (!kr.empty()) os << "const int k" << id << " = " << kr << ";\n";
         for (int i = 0; i < NR; ++i) {
             int rk = 0;
             for (int d = 0; d < J; ++d)
@@ -770,7 +816,7 @@ struct Gen {
         const int M = op.reg, q = local_of_reg(M);
         if (dep_count(q) > kMaxVariantBits) flush_all();
         os << "{\n";
-        const PairPhase P = take_phase(q, sp.lam);
+        const PairPhase P = take_phase(q, sp.lam, true);
         const int ts = slot(sp.t);
         os << "const " << T << " t = " << av(ts) << ";\n";
         for (int i = 0; i < NR; ++i) {
@@ -781,7 +827,18 @@ struct Gen {
                 os << "const " << T << " wr = " << X(k) << ", wi = " << Y(k) << ";\n";
             else if (P.cls == 1)
                 os << "const " << T << " wr = -" << X(k) << ", wi = -" << Y(k) << ";\n";
-            else
+            else if (P.shear[i]) {
+                // w = i^quad exp(i a) y: (ur, ui) = i^quad y (a renaming, its signs folded into the
+                // multiply-adds), then three shears, 3 FMAs against 4 for the complex product
+                static const char* const ur_of[4] = {"", "-", "-", ""};
+                static const char* const ui_of[4] = {"", "", "-", "-"};
+                const int qd = P.quad[i];
+                const std::string ur = std::string(ur_of[qd]) + ((qd & 1) ? Y(k) : X(k));
+                const std::string ui = std::string(ui_of[qd]) + ((qd & 1) ? X(k) : Y(k));
+                os << "const " << T << " pu = " << ur << " - " << P.re[i] << " * " << ui << ";\n";
+                os << "const " << T << " wi = " << ui << " + " << P.im[i] << " * pu;\n";
+                os << "const " << T << " wr = pu - " << P.re[i] << " * wi;\n";
+            } else
                 os << "const " << T << " wr = " << P.re[i] << " * " << X(k) << " - " << P.im[i] << " * " << Y(k)
                    << ", wi = " << P.re[i] << " * " << Y(k) << " + " << P.im[i] << " * " << X(k) << ";\n";
             if (!sp.form_b)
