@@ -854,6 +854,16 @@ struct Gen {
         G *= sp.gm;
     }
 
+    // A CNOT folded into H CZ H (the H's went into the ops on its target before and after it):
+    // CZ(c, t) = exp(i pi c t) deferred as the parity phases i^c, i^t and (-i)^(c xor t).
+    void cz(const FusedOp& op) {
+        const uint32_t t = 1u << local_of_reg(op.reg);
+        pend.push_back({op.cmask_local, op.cmask_outer, cplx(0.0, 1.0)});
+        pend.push_back({t, 0u, cplx(0.0, 1.0)});
+        pend.push_back({t | op.cmask_local, op.cmask_outer, cplx(0.0, -1.0)});
+        normalize();
+    }
+
     void op(int o, const FusedOp& op) {
         uint32_t rm, tb;
         split(op.cmask_local, rm, tb);
@@ -967,6 +977,91 @@ struct Generated {
     int hist_bins = 0;               // joint-mass epilogue bins (0: none)
     bool zero_start = false;         // the pass writes |0...0> instead of loading the state
 };
+
+// CNOT folding (QM_CZ_FOLD=0 turns it off).  A CNOT whose one control is a thread bit or a bit
+// outside the block, with its target t in a register, is a conditional register swap: four
+// selects per amplitude pair.  Since CNOT = H_t CZ H_t, where the op before it on t and the op
+// after it on t (within the pass) are both uncontrolled 2x2 unitaries U_p and U_n, they become
+// H U_p and U_n H (still rotations, at the same cost), and the CNOT becomes CZ(c, t), which the
+// generator defers as three parity phases (exp(i pi c t) = i^c i^t (-i)^(c xor t)): no
+// instruction at the CNOT.  `cz` marks the folded CNOTs and `forced` the ops whose coefficients
+// changed: those must run as rotations (their constants travel in the kernel parameter; the
+// staged program keeps the original coefficients, which the interpreter runs whole).
+bool cz_fold_enabled() {
+    const char* e = std::getenv("QM_CZ_FOLD");
+    return !(e && e[0] == '0');
+}
+
+void fold_controlled_x(const FusedPass& p, std::vector<FusedOp>& ops, std::vector<char>& cz, std::vector<char>& forced) {
+    const int n = (int)ops.size();
+    cz.assign((size_t)n, 0);
+    forced.assign((size_t)n, 0);
+    // local bits each op touches (a stage touches none; anything unknown touches all)
+    std::vector<uint32_t> touch((size_t)n, 0), regs((size_t)n, 0);
+    int8_t pos[R];
+    for (int m = 0; m < R; ++m) pos[m] = p.reg_in[m];
+    for (int o = 0; o < n; ++o) {
+        const FusedOp& op = ops[(size_t)o];
+        uint32_t rm = 0;
+        for (int m = 0; m < R; ++m) rm |= 1u << pos[m];
+        regs[(size_t)o] = rm;
+        uint32_t t = op.cmask_local;
+        switch (op.code) {
+        case OP_STAGE:
+            for (int m = 0; m < R; ++m) pos[m] = op.reg_pos[m];
+            t = 0;
+            break;
+        case OP_MATRIX:
+        case OP_MATRIX_REAL:
+        case OP_EXCHANGE: t |= 1u << pos[op.reg]; break;
+        case OP_SWAP: t |= (1u << pos[op.reg]) | (1u << pos[op.reg2]); break;
+        case OP_DIAG:
+            if (op.local >= 0) t |= 1u << op.local;
+            break;
+        case OP_NEGATE:
+        case OP_DIAG_GROUP: break;  // a group's members follow as ops of their own
+        default: t = ~0u;
+        }
+        touch[(size_t)o] = t;
+    }
+    const double h = std::sqrt(0.5);
+    auto plain = [&](int o) {
+        const FusedOp& op = ops[(size_t)o];
+        return (op.code == OP_MATRIX || op.code == OP_MATRIX_REAL) && op.cmask_local == 0 && op.cmask_outer == 0 &&
+               !(op.flags & (kOpTable | kOpBranch));
+    };
+    for (int o = 0; o < n; ++o) {
+        const FusedOp& x = ops[(size_t)o];
+        if (x.code != OP_EXCHANGE) continue;
+        if (__builtin_popcount(x.cmask_local) + __builtin_popcount(x.cmask_outer) != 1) continue;
+        if (x.cmask_local & regs[(size_t)o]) continue;  // a register control is a free renaming
+        const uint32_t tb = touch[(size_t)o] & ~x.cmask_local;
+        int before = -1, after = -1;
+        for (int j = o - 1; j >= 0 && before < 0; --j)
+            if (touch[(size_t)j] & tb) before = j;
+        for (int j = o + 1; j < n && after < 0; ++j)
+            if (touch[(size_t)j] & tb) after = j;
+        if (before < 0 || after < 0 || !plain(before) || !plain(after)) continue;
+        // H U (rows mixed) for the op before, U H (columns mixed) for the op after
+        double* u = ops[(size_t)before].coef;
+        double* v = ops[(size_t)after].coef;
+        double nu[8], nv[8];
+        for (int k = 0; k < 4; ++k) {
+            nu[k] = h * (u[k] + u[k + 4]);
+            nu[k + 4] = h * (u[k] - u[k + 4]);
+        }
+        for (int r = 0; r < 2; ++r)
+            for (int k = 0; k < 2; ++k) {
+                nv[4 * r + k] = h * (v[4 * r + k] + v[4 * r + 2 + k]);
+                nv[4 * r + 2 + k] = h * (v[4 * r + k] - v[4 * r + 2 + k]);
+            }
+        if (!split_unitary(nu).ok || !split_unitary(nv).ok) continue;
+        std::copy(nu, nu + 8, u);
+        std::copy(nv, nv + 8, v);
+        cz[(size_t)o] = 1;
+        forced[(size_t)before] = forced[(size_t)after] = 1;
+    }
+}
 
 Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int qubits, bool fp64, Carry* carry,
                    bool last, uint32_t hist_mask = 0, bool zero_start = false) {
@@ -1161,8 +1256,19 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int
         os << "}\n";
         os << "u32 base = " << g.base_expr() << ";\n";
     }
+    std::vector<FusedOp> pass_ops(plan_ops.begin() + p.op_begin, plan_ops.begin() + p.op_begin + p.op_count);
+    std::vector<char> as_cz, forced;
+    if (cz_fold_enabled()) fold_controlled_x(p, pass_ops, as_cz, forced);
     for (int o = 0; o < p.op_count; ++o) {
-        const FusedOp& op = plan_ops[(size_t)(p.op_begin + o)];
+        const FusedOp& op = pass_ops[(size_t)o];
+        if (!as_cz.empty() && as_cz[(size_t)o]) {
+            g.cz(op);
+            continue;
+        }
+        if (!forced.empty() && forced[(size_t)o]) {
+            g.rotation(op, split_unitary(op.coef));
+            continue;
+        }
         if (op.code == OP_STAGE) {
             os << release;
             g.stage(op.reg_pos, op.reserved);
