@@ -133,3 +133,28 @@ def test_pipelined_passes(gpu_context):
     assert np.max(np.abs(out[FP64] - want)) <= 1e-12
     rel = np.linalg.norm(out[FP32] - out[FP64]) / np.linalg.norm(out[FP64])
     assert rel <= 1e-5
+
+
+@pytest.mark.gpu
+def test_pipelined_passes_as_two_teams(gpu_context, monkeypatch):
+    """With QM_TEAMS=1 complex128 pipelined passes run as one 512-thread block per SM of two
+    teams that hand a compute token back and forth by named barriers (blocks whose second team
+    has no work item included); the state must match the oracle's parallel path."""
+    monkeypatch.setenv("QM_TEAMS", "1")
+    n = 26
+    c = brick_circuit(n, 4, seed=5)
+    want = orc.execute_parallel(c)
+    g, count = prepare(c)
+    ln = C.c_size_t()
+    check(load().qm_jit_source(n, FP64, g, count, 0, 0, None, 0, C.byref(ln)))
+    buf = C.create_string_buffer(ln.value + 1)
+    check(load().qm_jit_source(n, FP64, g, count, 0, 0, buf, ln.value + 1, C.byref(ln)))
+    assert b"const u32 team = threadIdx.x >>" in buf.value
+    p = Plan(gpu_context, c, FP64, 0)
+    try:
+        with DeviceState(gpu_context, n, FP64) as st:
+            p.execute(st)
+            got = st.Download()
+    finally:
+        p.Dispose()
+    assert np.max(np.abs(got - want)) <= 1e-12
