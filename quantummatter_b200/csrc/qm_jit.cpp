@@ -983,7 +983,7 @@ struct Generated {
 // CNOT folding (QM_CZ_FOLD=0 turns it off).  A CNOT whose one control is a thread bit or a bit
 // outside the block, with its target t in a register, is a conditional register swap: four
 // selects per amplitude pair.  Since CNOT = H_t CZ H_t, where the op before it on t and the op
-// after it on t (within the pass) are both uncontrolled 2x2 unitaries U_p and U_n, they become
+// after it on t (in the plan) are both uncontrolled 2x2 unitaries U_p and U_n, they become
 // H U_p and U_n H (still rotations, at the same cost), and the CNOT becomes CZ(c, t), which the
 // generator defers as three parity phases (exp(i pi c t) = i^c i^t (-i)^(c xor t)): no
 // instruction at the CNOT.  `cz` marks the folded CNOTs and `forced` the ops whose coefficients
@@ -994,79 +994,135 @@ bool cz_fold_enabled() {
     return !(e && e[0] == '0');
 }
 
-void fold_controlled_x(const FusedPass& p, std::vector<FusedOp>& ops, std::vector<char>& cz, std::vector<char>& forced) {
-    const int n = (int)ops.size();
-    cz.assign((size_t)n, 0);
-    forced.assign((size_t)n, 0);
-    // local bits each op touches (a stage touches none; anything unknown touches all)
-    std::vector<uint32_t> touch((size_t)n, 0), regs((size_t)n, 0);
-    int8_t pos[R];
-    for (int m = 0; m < R; ++m) pos[m] = p.reg_in[m];
-    for (int o = 0; o < n; ++o) {
-        const FusedOp& op = ops[(size_t)o];
-        uint32_t rm = 0;
-        for (int m = 0; m < R; ++m) rm |= 1u << pos[m];
-        regs[(size_t)o] = rm;
-        uint32_t t = op.cmask_local;
-        switch (op.code) {
-        case OP_STAGE:
-            for (int m = 0; m < R; ++m) pos[m] = op.reg_pos[m];
-            t = 0;
-            break;
-        case OP_MATRIX:
-        case OP_MATRIX_REAL:
-        case OP_EXCHANGE: t |= 1u << pos[op.reg]; break;
-        case OP_SWAP: t |= (1u << pos[op.reg]) | (1u << pos[op.reg2]); break;
-        case OP_DIAG:
-            if (op.local >= 0) t |= 1u << op.local;
-            break;
-        case OP_NEGATE:
-        case OP_DIAG_GROUP: break;  // a group's members follow as ops of their own
-        default: t = ~0u;
+// The plan's ops with the folds applied: `cz` marks the folded CNOTs, `forced` the ops whose
+// coefficients changed.  With `across` (chained plans, whose passes all run compiled) the op
+// before or after a CNOT on its target may lie in another pass: qubits are followed through each
+// pass's relabeling store (local bit b read from index bit q[b], written to q_out[b]).  Without
+// it only folds within one pass are made, so a pass that runs on the interpreter (the original
+// ops) never meets a neighbour changed for it.
+struct Fold {
+    std::vector<FusedOp> ops;
+    std::vector<char> cz, forced;
+};
+
+Fold fold_plan(const Plan& plan, bool across) {
+    Fold f;
+    f.ops = plan.ops;
+    f.cz.assign(plan.ops.size(), 0);
+    f.forced.assign(plan.ops.size(), 0);
+    if (!cz_fold_enabled() || plan.qubits > 32) return f;
+    // per op: its pass, the logical qubits it touches (~0: unknown, touches all), and for a CNOT
+    // candidate its target's logical qubit
+    const size_t n = plan.ops.size();
+    std::vector<int> pass_of(n, -1), target(n, -1);
+    std::vector<uint64_t> touch(n, 0);
+    int phys_to_log[32], log_to_phys[32];
+    for (int q = 0; q < 32; ++q) phys_to_log[q] = log_to_phys[q] = q;
+    auto logical = [&](uint32_t phys_mask) {
+        uint64_t m = 0;
+        for (int q = 0; q < 32; ++q)
+            if ((phys_mask >> q) & 1u) m |= uint64_t(1) << phys_to_log[q];
+        return m;
+    };
+    for (size_t pi = 0; pi < plan.passes.size(); ++pi) {
+        const FusedPass& p = plan.passes[pi];
+        int8_t pos[R];
+        for (int m = 0; m < R; ++m) pos[m] = p.reg_in[m];
+        auto local_logical = [&](uint32_t local_mask) {
+            uint32_t phys = 0;
+            for (int b = 0; b < p.k; ++b)
+                if ((local_mask >> b) & 1u) phys |= 1u << p.q[b];
+            return logical(phys);
+        };
+        for (int o = 0; o < p.op_count; ++o) {
+            const size_t gi = (size_t)(p.op_begin + o);
+            const FusedOp& op = plan.ops[gi];
+            pass_of[gi] = (int)pi;
+            uint32_t rm = 0;
+            for (int m = 0; m < R; ++m) rm |= 1u << pos[m];
+            uint32_t loc = op.cmask_local;
+            uint64_t t = 0;
+            switch (op.code) {
+            case OP_STAGE:
+                for (int m = 0; m < R; ++m) pos[m] = op.reg_pos[m];
+                loc = 0;
+                break;
+            case OP_MATRIX:
+            case OP_MATRIX_REAL:
+            case OP_EXCHANGE: loc |= 1u << pos[op.reg]; break;
+            case OP_SWAP: loc |= (1u << pos[op.reg]) | (1u << pos[op.reg2]); break;
+            case OP_DIAG:
+                if (op.local >= 0) loc |= 1u << op.local;
+                break;
+            case OP_NEGATE:
+            case OP_DIAG_GROUP: break;  // a group's members follow as ops of their own
+            default: t = ~uint64_t(0);
+            }
+            if (op.code != OP_STAGE) t |= local_logical(loc) | logical(op.cmask_outer | op.target_outer);
+            touch[gi] = t;
+            if (op.code == OP_EXCHANGE && __builtin_popcount(op.cmask_local) + __builtin_popcount(op.cmask_outer) == 1 &&
+                !(op.cmask_local & rm))
+                target[gi] = (int)__builtin_ctzll(local_logical(1u << pos[op.reg]));
         }
-        touch[(size_t)o] = t;
+        // the store: the logical qubit read from index bit q[b] now sits at q_out[b]
+        int moved[32];
+        for (int q = 0; q < 32; ++q) moved[q] = phys_to_log[q];
+        for (int b = 0; b < p.k; ++b) moved[p.q_out[b]] = phys_to_log[p.q[b]];
+        for (int q = 0; q < 32; ++q) {
+            phys_to_log[q] = moved[q];
+            log_to_phys[moved[q]] = q;
+        }
     }
+    // ops in plan order (passes are laid out in order in the op array)
+    std::vector<size_t> order;
+    for (const FusedPass& p : plan.passes)
+        for (int o = 0; o < p.op_count; ++o) order.push_back((size_t)(p.op_begin + o));
     const double h = std::sqrt(0.5);
-    auto plain = [&](int o) {
-        const FusedOp& op = ops[(size_t)o];
+    auto plain = [&](size_t gi) {
+        const FusedOp& op = f.ops[gi];
         return (op.code == OP_MATRIX || op.code == OP_MATRIX_REAL) && op.cmask_local == 0 && op.cmask_outer == 0 &&
                !(op.flags & (kOpTable | kOpBranch));
     };
-    for (int o = 0; o < n; ++o) {
-        const FusedOp& x = ops[(size_t)o];
-        if (x.code != OP_EXCHANGE) continue;
-        if (__builtin_popcount(x.cmask_local) + __builtin_popcount(x.cmask_outer) != 1) continue;
-        if (x.cmask_local & regs[(size_t)o]) continue;  // a register control is a free renaming
-        const uint32_t tb = touch[(size_t)o] & ~x.cmask_local;
-        int before = -1, after = -1;
-        for (int j = o - 1; j >= 0 && before < 0; --j)
-            if (touch[(size_t)j] & tb) before = j;
-        for (int j = o + 1; j < n && after < 0; ++j)
-            if (touch[(size_t)j] & tb) after = j;
-        if (before < 0 || after < 0 || !plain(before) || !plain(after)) continue;
+    for (size_t k = 0; k < order.size(); ++k) {
+        const size_t gi = order[k];
+        if (target[gi] < 0) continue;
+        const uint64_t tb = uint64_t(1) << target[gi];
+        long before = -1, after = -1;
+        for (long j = (long)k - 1; j >= 0 && before < 0; --j) {
+            if (!across && pass_of[order[(size_t)j]] != pass_of[gi]) break;
+            if (touch[order[(size_t)j]] & tb) before = j;
+        }
+        for (size_t j = k + 1; j < order.size() && after < 0; ++j) {
+            if (!across && pass_of[order[j]] != pass_of[gi]) break;
+            if (touch[order[j]] & tb) after = (long)j;
+        }
+        if (before < 0 || after < 0) continue;
+        const size_t bi = order[(size_t)before], ai = order[(size_t)after];
+        if (!plain(bi) || !plain(ai)) continue;
         // H U (rows mixed) for the op before, U H (columns mixed) for the op after
-        double* u = ops[(size_t)before].coef;
-        double* v = ops[(size_t)after].coef;
+        double* u = f.ops[bi].coef;
+        double* v = f.ops[ai].coef;
         double nu[8], nv[8];
-        for (int k = 0; k < 4; ++k) {
-            nu[k] = h * (u[k] + u[k + 4]);
-            nu[k + 4] = h * (u[k] - u[k + 4]);
+        for (int c = 0; c < 4; ++c) {
+            nu[c] = h * (u[c] + u[c + 4]);
+            nu[c + 4] = h * (u[c] - u[c + 4]);
         }
         for (int r = 0; r < 2; ++r)
-            for (int k = 0; k < 2; ++k) {
-                nv[4 * r + k] = h * (v[4 * r + k] + v[4 * r + 2 + k]);
-                nv[4 * r + 2 + k] = h * (v[4 * r + k] - v[4 * r + 2 + k]);
+            for (int c = 0; c < 2; ++c) {
+                nv[4 * r + c] = h * (v[4 * r + c] + v[4 * r + 2 + c]);
+                nv[4 * r + 2 + c] = h * (v[4 * r + c] - v[4 * r + 2 + c]);
             }
         if (!split_unitary(nu).ok || !split_unitary(nv).ok) continue;
         std::copy(nu, nu + 8, u);
         std::copy(nv, nv + 8, v);
-        cz[(size_t)o] = 1;
-        forced[(size_t)before] = forced[(size_t)after] = 1;
+        f.cz[gi] = 1;
+        f.forced[bi] = f.forced[ai] = 1;
     }
+    return f;
 }
 
-Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int qubits, bool fp64, Carry* carry,
-                   bool last, uint32_t hist_mask = 0, bool zero_start = false) {
+Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, const Fold& fold, int qubits, bool fp64,
+                   Carry* carry, bool last, uint32_t hist_mask = 0, bool zero_start = false) {
     Gen g;
     g.fp64 = fp64;
     g.K = p.k;
@@ -1258,16 +1314,14 @@ Generated generate(const FusedPass& p, const std::vector<FusedOp>& plan_ops, int
         os << "}\n";
         os << "u32 base = " << g.base_expr() << ";\n";
     }
-    std::vector<FusedOp> pass_ops(plan_ops.begin() + p.op_begin, plan_ops.begin() + p.op_begin + p.op_count);
-    std::vector<char> as_cz, forced;
-    if (cz_fold_enabled()) fold_controlled_x(p, pass_ops, as_cz, forced);
     for (int o = 0; o < p.op_count; ++o) {
-        const FusedOp& op = pass_ops[(size_t)o];
-        if (!as_cz.empty() && as_cz[(size_t)o]) {
+        const size_t gi = (size_t)(p.op_begin + o);
+        const FusedOp& op = fold.ops[gi];
+        if (fold.cz[gi]) {
             g.cz(op);
             continue;
         }
-        if (!forced.empty() && forced[(size_t)o]) {
+        if (fold.forced[gi]) {
             g.rotation(op, split_unitary(op.coef));
             continue;
         }
@@ -1419,8 +1473,9 @@ std::vector<Generated> generate_plan(const Plan& plan, bool chained) {
     std::vector<Generated> out;
     out.reserve(plan.passes.size());
     Carry carry;
+    const Fold fold = fold_plan(plan, chained);
     for (size_t i = 0; i < plan.passes.size(); ++i)
-        out.push_back(generate(plan.passes[i], plan.ops, plan.qubits, fp64, chained ? &carry : nullptr,
+        out.push_back(generate(plan.passes[i], plan.ops, fold, plan.qubits, fp64, chained ? &carry : nullptr,
                                i + 1 == plan.passes.size(), i + 1 == plan.passes.size() ? plan.hist_mask : 0u,
                                i == 0 && plan.start_zero));
     return out;
