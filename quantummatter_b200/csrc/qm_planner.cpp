@@ -18,6 +18,7 @@
 // pass reads whole) hold the qubits the next pass can use best; the last passes restore the order.
 // Such a plan is kept only when it needs fewer passes than the plain one.
 #include <algorithm>
+#include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <string>
@@ -738,8 +739,72 @@ bool plan_fused_with(const std::vector<qm_gate>& gates, int qubits, int precisio
 // Plans without relabeling and, where relabeling applies, with it: the relabeling plan is kept
 // only when it needs fewer passes, since its lane stages and restoring pass cost more than they
 // save otherwise.
-bool plan_fused(const std::vector<qm_gate>& gates, int qubits, int precision, int width, Plan& plan,
+// CNOTs rewritten as CZs for fused blocks (QM_CZ_REWRITE=0 turns it off).  CNOT(c, t) =
+// H_t CZ(c, t) H_t; where the gates before and after it on t are uncontrolled single-qubit
+// matrices U_p and U_n, they become H U_p and U_n H and the CNOT a CZ.  A CZ is diagonal, so a
+// stage need not hold t in a register for it and gates commute past it on c and t alike: the
+// 30-qubit brick plans in 25 passes of 142 stages instead of 29 of 185 (complex64: 23 of 130
+// instead of 34 of 191).  Exact up to the rounding of the two matrix products.
+bool cz_rewrite_enabled() {
+    const char* e = std::getenv("QM_CZ_REWRITE");
+    return !(e && e[0] == '0');
+}
+
+std::vector<qm_gate> cnots_as_cz(const std::vector<qm_gate>& gates) {
+    std::vector<qm_gate> out(gates);
+    const size_t n = out.size();
+    auto touches = [](const qm_gate& g, int q) {
+        return g.target == q || ((g.control_mask >> q) & 1u) || g.swap_control == q;
+    };
+    auto plain = [](const qm_gate& g) {
+        return (g.kernel == QM_KERNEL_MATRIX || g.kernel == QM_KERNEL_HADAMARD) && g.control_mask == 0 &&
+               g.swap_control < 0;
+    };
+    const double h = std::sqrt(0.5);
+    for (size_t i = 0; i < n; ++i) {
+        const qm_gate& x = out[i];
+        if (x.kernel != QM_KERNEL_EXCHANGE || __builtin_popcount(x.control_mask) != 1 || x.swap_control >= 0) continue;
+        const int t = x.target;
+        long before = -1, after = -1;
+        for (long j = (long)i - 1; j >= 0 && before < 0; --j)
+            if (touches(out[(size_t)j], t)) before = j;
+        for (size_t j = i + 1; j < n && after < 0; ++j)
+            if (touches(out[j], t)) after = (long)j;
+        if (before < 0 || after < 0 || !plain(out[(size_t)before]) || !plain(out[(size_t)after])) continue;
+        qm_gate& u = out[(size_t)before];
+        qm_gate& v = out[(size_t)after];
+        // H U: rows (a, b) and (c, d) mixed; U H: columns (a, c) and (b, d) mixed
+        for (int k = 0; k < 2; ++k) {
+            const double a = u.a[k], b = u.b[k], c = u.c[k], d = u.d[k];
+            u.a[k] = h * (a + c);
+            u.b[k] = h * (b + d);
+            u.c[k] = h * (a - c);
+            u.d[k] = h * (b - d);
+            const double va = v.a[k], vb = v.b[k], vc = v.c[k], vd = v.d[k];
+            v.a[k] = h * (va + vb);
+            v.b[k] = h * (va - vb);
+            v.c[k] = h * (vc + vd);
+            v.d[k] = h * (vc - vd);
+        }
+        u.kernel = QM_KERNEL_MATRIX;
+        v.kernel = QM_KERNEL_MATRIX;
+        qm_gate& z = out[i];
+        z.kernel = QM_KERNEL_DIAGONAL;
+        z.a[0] = 1.0;
+        z.a[1] = 0.0;
+        z.b[0] = z.b[1] = z.c[0] = z.c[1] = 0.0;
+        z.d[0] = -1.0;
+        z.d[1] = 0.0;
+    }
+    return out;
+}
+
+bool plan_fused(const std::vector<qm_gate>& in, int qubits, int precision, int width, Plan& plan,
                 std::string& error, const std::vector<int32_t>* slots) {
+    std::vector<qm_gate> rewritten;
+    const bool rewrite = !slots && cz_rewrite_enabled() && (width == 0 || width >= 9);
+    if (rewrite) rewritten = cnots_as_cz(in);
+    const std::vector<qm_gate>& gates = rewrite ? rewritten : in;
     if (!plan_fused_with(gates, qubits, precision, width, plan, error, slots, false)) return false;
     if (slots || !relabel_enabled() || plan.width == 1 || plan.passes.size() < 2) return true;
     Plan alt;

@@ -189,12 +189,13 @@ def _lowest_ranks(registers, lanes, k, n):
     return (list(lanes) + free)[:n]
 
 
-@pytest.mark.parametrize("precision,low,allowed", [(0, 3, 0.0), (1, 4, 0.1)], ids=["fp64", "fp32"])
+@pytest.mark.parametrize("precision,low,allowed", [(0, 3, 0.02), (1, 4, 0.1)], ids=["fp64", "fp32"])
 def test_exchanges_keep_shared_memory_free_of_bank_conflicts(precision, low, allowed):
     """An exchange goes through shared memory in phases of 2^low threads (ranks 0..low-1) and the
-    swizzle sends local bit p to bank-group bit p mod low: every exchange side but a relabeling
-    pass's final lanes (fixed by the store) holds bits of distinct classes on those ranks
-    (complex64 stages may lack a class among their free bits)."""
+    swizzle sends local bit p to bank-group bit p mod low: nearly every exchange side but a
+    relabeling pass's final lanes (fixed by the store) holds bits of distinct classes on those
+    ranks (stages may lack a class among their free bits: 2 of 209 complex128 sides of the brick
+    once its CNOTs plan as CZs)."""
     c = brick_circuit(30, 40)
     gates, count = prepare(c)
     passes, ops, _ = pe.program(30, precision, gates, count, 0)
