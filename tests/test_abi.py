@@ -315,3 +315,25 @@ def test_no_device_behaviour_on_a_cpu_host():
     h = C.c_void_p()
     assert lib.qm_context_create(C.byref(o), C.byref(h)) == 4
     assert "No compatible NVIDIA CUDA device" in _lib.last_error()
+
+
+def test_cnots_between_single_qubit_matrices_plan_as_cz(monkeypatch):
+    """CNOT(c, t) = H_t CZ(c, t) H_t: where the gates before and after a CNOT on its target are
+    single-qubit matrices, the planner merges the Hadamards into them and plans a CZ, a diagonal
+    that needs no register for t.  The 30-qubit brick then plans in 25 passes instead of 29 (566
+    of its 580 CNOTs; the last layer's have no gate after them); QM_CZ_REWRITE=0 keeps the
+    CNOTs.  The rewritten plans reproduce the oracle."""
+    c = brick_circuit(30, 40)
+    gates, count = prepare(c)
+
+    def counts():
+        passes, ops, _ = pe.program(30, 0, gates, count, 0)
+        return len(passes), sum(o.code == 3 for o in ops), sum(o.code == 5 for o in ops)
+
+    assert counts() == (25, 14, 566)
+    monkeypatch.setenv("QM_CZ_REWRITE", "0")
+    assert counts()[:2] == (29, 580)
+    monkeypatch.delenv("QM_CZ_REWRITE")
+    for seed in range(3):
+        _emulate_against_oracle(brick_circuit(16, 12, seed=seed), 0, seed=seed)
+        _emulate_against_oracle(random_circuit(14, 300, seed=40 + seed), 0, seed=seed)
