@@ -903,8 +903,10 @@ def main() -> None:
     # amplitude for a general unitary (a scaled rotation between deferred phases), 4 for a real one.
     dense = sum(1 for op in circuit.Operations if int(op.Kind) in (0, 6, 7, 15))
     flops = dense * amps * 8 * 2
-    # what the compiled passes issue: 8 flops per amplitude for a general 2x2 (Rx, U), 4 for a real
-    # one (H, Ry), against the FP64 peak of 64 FMA per clock per SM at the sampled SM clock
+    # what the compiled passes issue, counting an FMA as 2 flops: at most 8 per amplitude for a
+    # general 2x2 (Rx, U; 7 where the rotation's phase is known at compile time and applied by
+    # three shears), 4 for a real one (H, Ry), against the FP64 peak of 64 FMA per clock per SM at
+    # the sampled SM clock; the ncu pipe counter beside it is the measured side
     fp64_flops = amps * sum(8 if int(op.Kind) in (6, 15) else 4
                             for op in circuit.Operations if int(op.Kind) in (0, 6, 7, 15))
     e2e = None
