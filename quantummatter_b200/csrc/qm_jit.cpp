@@ -715,9 +715,37 @@ struct Gen {
             }
             return P;
         }
+        // Phases chosen at run time take the shear form too when one quadrant i^quad leaves every
+        // variant within 3 pi / 4 of it (shear constants up to tan(3 pi / 8) = 2.41): the table
+        // then holds each variant's (tan(a / 2), sin(a)) instead of (re, im).
+        int rquad = -1;
+        if (shears) {
+            double best = 3 * M_PI / 4 + 1e-12;
+            for (int qd = 0; qd < 4; ++qd) {
+                double worst = 0.0;
+                for (int key = 0; key < (1 << J); ++key) {
+                    const double a = std::remainder(std::arg(variant(key)) - qd * (M_PI / 2), 2 * M_PI);
+                    worst = std::max(worst, std::fabs(a));
+                }
+                if (worst < best) {
+                    best = worst;
+                    rquad = qd;
+                }
+            }
+        }
         const int first = (int)aux.size();
-        for (int key = 0; key < (1 << J); ++key) slot2(variant(key));
+        for (int key = 0; key < (1 << J); ++key) {
+            if (rquad < 0) {
+                slot2(variant(key));
+            } else {
+                const double a = std::remainder(std::arg(variant(key)) - rquad * (M_PI / 2), 2 * M_PI);
+                slot(std::tan(a / 2));
+                slot(std::sin(a));
+            }
+        }
         if (!kr.empty()) os << "const int k" << id << " = " << kr << ";\n";
+        const char* c0 = rquad < 0 ? "r" : "a";
+        const char* c1 = rquad < 0 ? "i" : "b";
         for (int i = 0; i < NR; ++i) {
             int rk = 0;
             for (int d = 0; d < J; ++d)
@@ -726,11 +754,16 @@ struct Gen {
                 const std::string n = "l" + id + "_" + std::to_string(rk);
                 const std::string at = kr.empty() ? std::to_string(first + 2 * rk)
                                                   : std::to_string(first) + " + 2 * (k" + id + " ^ " + std::to_string(rk) + ")";
-                os << "const " << T << " " << n << "r = A.v[" << at << "], " << n << "i = A.v[" << at << " + 1];\n";
+                os << "const " << T << " " << n << c0 << " = A.v[" << at << "], " << n << c1 << " = A.v[" << at
+                   << " + 1];\n";
                 declared[rk] = n;
             }
-            P.re[i] = declared[rk] + "r";
-            P.im[i] = declared[rk] + "i";
+            P.re[i] = declared[rk] + c0;
+            P.im[i] = declared[rk] + c1;
+            if (rquad >= 0) {
+                P.shear[i] = true;
+                P.quad[i] = rquad;
+            }
         }
         return P;
     }
