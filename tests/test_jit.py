@@ -158,3 +158,41 @@ def test_pipelined_passes_as_two_teams(gpu_context, monkeypatch):
     finally:
         p.Dispose()
     assert np.max(np.abs(got - want)) <= 1e-12
+
+
+def _sources(circuit, precision=FP64):
+    g, n = prepare(circuit)
+    out, p = [], 0
+    while True:
+        ln = C.c_size_t()
+        if load().qm_jit_source(circuit.QubitCount, precision, g, n, 0, p, None, 0, C.byref(ln)):
+            return out
+        buf = C.create_string_buffer(ln.value + 1)
+        check(load().qm_jit_source(circuit.QubitCount, precision, g, n, 0, p, buf, ln.value + 1, C.byref(ln)))
+        out.append(buf.value.decode())
+        p += 1
+
+
+def test_generated_forms_of_the_benchmark_circuit(monkeypatch):
+    """The 30-qubit brick's passes: every rotation pair applies its phase by three shears (7 FMAs
+    per pair), the CNOTs planned as CZs leave no conditional register swap behind but those of the
+    last layer, and the CZ signs are deferred into the rotations' phases.  The real-rotation
+    ansatz (Ry, Rz, CZ ladders) keeps its CZs as negations, which deferral would turn into complex
+    products."""
+    from quantummatter_b200.workloads import hardware_efficient_ansatz, uniform_parameters
+    src = _sources(brick_circuit(30, 40))
+    assert len(src) == 25
+    text = "\n".join(src)
+    shears = text.count("const double wr = pu")
+    products = len(re.findall(r"const double wr = \w+ \* x", text))
+    assert shears > 9000 and products == 0
+    assert text.count("double u = x") <= 8 * 14  # conditional swaps: at most the last layer's CNOTs
+    monkeypatch.setenv("QM_CZ_DEFER", "0")
+    negations_off = "\n".join(_sources(brick_circuit(30, 40))).count("= -x")
+    monkeypatch.delenv("QM_CZ_DEFER")
+    assert text.count("= -x") < negations_off
+    a = hardware_efficient_ansatz(22, 4)
+    bound = a.Bind(list(uniform_parameters(a.ParameterCount, 1, -3, 3, seed=1)[0]))
+    on = "\n".join(_sources(bound)).count("= -x")
+    monkeypatch.setenv("QM_CZ_DEFER", "0")
+    assert on == "\n".join(_sources(bound)).count("= -x")
