@@ -1207,20 +1207,34 @@ Fold fold_plan(const Plan& plan, bool across) {
         return (op.code == OP_MATRIX || op.code == OP_MATRIX_REAL) && op.cmask_local == 0 && op.cmask_outer == 0 &&
                !(op.flags & (kOpTable | kOpBranch));
     };
-    for (size_t k = 0; k < order.size(); ++k) {
+    // the previous and next op touching each candidate's target, in plan order (folding keeps
+    // every op's qubits)
+    const size_t m = order.size();
+    std::vector<long> prev_on(m, -1), next_on(m, -1);
+    {
+        long last[64];
+        std::fill(last, last + 64, -1L);
+        for (size_t k = 0; k < m; ++k) {
+            const size_t gi = order[k];
+            if (target[gi] >= 0) prev_on[k] = last[target[gi]];
+            for (int q = 0; q < 64; ++q)
+                if ((touch[gi] >> q) & 1u) last[q] = (long)k;
+        }
+        std::fill(last, last + 64, -1L);
+        for (size_t k = m; k-- > 0;) {
+            const size_t gi = order[k];
+            if (target[gi] >= 0) next_on[k] = last[target[gi]];
+            for (int q = 0; q < 64; ++q)
+                if ((touch[gi] >> q) & 1u) last[q] = (long)k;
+        }
+    }
+    for (size_t k = 0; k < m; ++k) {
         const size_t gi = order[k];
         if (target[gi] < 0) continue;
-        const uint64_t tb = uint64_t(1) << target[gi];
-        long before = -1, after = -1;
-        for (long j = (long)k - 1; j >= 0 && before < 0; --j) {
-            if (!across && pass_of[order[(size_t)j]] != pass_of[gi]) break;
-            if (touch[order[(size_t)j]] & tb) before = j;
-        }
-        for (size_t j = k + 1; j < order.size() && after < 0; ++j) {
-            if (!across && pass_of[order[j]] != pass_of[gi]) break;
-            if (touch[order[j]] & tb) after = (long)j;
-        }
+        const long before = prev_on[k], after = next_on[k];
         if (before < 0 || after < 0) continue;
+        if (!across && (pass_of[order[(size_t)before]] != pass_of[gi] || pass_of[order[(size_t)after]] != pass_of[gi]))
+            continue;
         const size_t bi = order[(size_t)before], ai = order[(size_t)after];
         if (!plain(bi) || !plain(ai)) continue;
         // H U (rows mixed) for the op before, U H (columns mixed) for the op after

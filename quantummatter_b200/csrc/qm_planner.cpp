@@ -760,19 +760,30 @@ std::vector<qm_gate> cnots_as_cz(const std::vector<qm_gate>& gates) {
         return (g.kernel == QM_KERNEL_MATRIX || g.kernel == QM_KERNEL_HADAMARD) && g.control_mask == 0 &&
                g.swap_control < 0;
     };
+    // the previous and next gate on each CNOT's target (the rewrite keeps every gate's qubits)
+    std::vector<long> before(n, -1), after(n, -1);
+    {
+        long last[32];
+        std::fill(last, last + 32, -1L);
+        for (size_t i = 0; i < n; ++i) {
+            if (out[i].target >= 0 && out[i].target < 32) before[i] = last[out[i].target];
+            for (int q = 0; q < 32; ++q)
+                if (touches(out[i], q)) last[q] = (long)i;
+        }
+        std::fill(last, last + 32, -1L);
+        for (size_t i = n; i-- > 0;) {
+            if (out[i].target >= 0 && out[i].target < 32) after[i] = last[out[i].target];
+            for (int q = 0; q < 32; ++q)
+                if (touches(out[i], q)) last[q] = (long)i;
+        }
+    }
     const double h = std::sqrt(0.5);
     for (size_t i = 0; i < n; ++i) {
         const qm_gate& x = out[i];
         if (x.kernel != QM_KERNEL_EXCHANGE || __builtin_popcount(x.control_mask) != 1 || x.swap_control >= 0) continue;
-        const int t = x.target;
-        long before = -1, after = -1;
-        for (long j = (long)i - 1; j >= 0 && before < 0; --j)
-            if (touches(out[(size_t)j], t)) before = j;
-        for (size_t j = i + 1; j < n && after < 0; ++j)
-            if (touches(out[j], t)) after = (long)j;
-        if (before < 0 || after < 0 || !plain(out[(size_t)before]) || !plain(out[(size_t)after])) continue;
-        qm_gate& u = out[(size_t)before];
-        qm_gate& v = out[(size_t)after];
+        if (before[i] < 0 || after[i] < 0 || !plain(out[(size_t)before[i]]) || !plain(out[(size_t)after[i]])) continue;
+        qm_gate& u = out[(size_t)before[i]];
+        qm_gate& v = out[(size_t)after[i]];
         // H U: rows (a, b) and (c, d) mixed; U H: columns (a, c) and (b, d) mixed
         for (int k = 0; k < 2; ++k) {
             const double a = u.a[k], b = u.b[k], c = u.c[k], d = u.d[k];
