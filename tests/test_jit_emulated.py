@@ -124,3 +124,23 @@ def test_pipelined_passes_on_the_cpu_match_the_oracle(monkeypatch, name, precisi
     want = orc.execute(c, psi)
     got = je.run_plan(c, precision, psi, grid=grid)
     assert np.max(np.abs(got - want)) <= tol
+
+
+@pytest.mark.timeout(900)
+def test_twenty_qubit_brick_plan_on_the_cpu_matches_the_oracle():
+    """The benchmark circuit's structure at 20 qubits: eight qubits outside every block, relabeling
+    passes, the CNOTs planned as CZs with their signs deferred, rotations whose phase is chosen at
+    run time by thread and work-item parities (in the shear form), phases carried across passes."""
+    from quantummatter_b200.circuit import prepare
+    from plan_emulator import program
+    c = brick_circuit(20, 20, seed=12)
+    g, n = prepare(c)
+    passes, ops, _ = program(20, FP64, g, n, 0)
+    assert any(p.qubits_out[b] != p.qubits[b] for p in passes for b in range(p.block_qubits))
+    assert sum(o.code == 5 for o in ops) > sum(o.code == 3 for o in ops)  # CZs, few CNOTs left
+    src = je._text(je.load().qm_jit_source, 20, FP64, g, n, 0, 1).decode()
+    assert "2 * (k" in src and "const double pu" in src
+    psi = random_state(20, 6)
+    want = orc.execute(c, psi)
+    got = je.run_plan(c, FP64, psi)
+    assert np.max(np.abs(got - want)) <= 1e-12
